@@ -1,0 +1,493 @@
+// bp.cu -- BackProjectionFDK behind the C ABI (cudaBP/backprojection.cuh:246-271,
+// cudaBP/backprojectionFDK.cu:161-362).
+//
+// Device state per handle: the sub-volume in the reference's layout [x][y][zs] (zs fastest,
+// top slab then bottom slab, backprojectionFDK.cu:119-126), two staging buffers for host
+// views so the copy of batch k+1 overlaps the kernel of batch k (copy stream + events), the
+// per-view matrices, and the kernel timer.
+#include <cuda_fp16.h>
+
+#include <chrono>
+#include <thread>
+#include <vector>
+
+#include "bp_exact.cuh"
+#include "bp_fast.cuh"
+#include "common.h"
+
+namespace fdk {
+
+// [x][y][zs] -> [zs][y][x] for zs in [z_begin, z_begin + dz), x fastest
+// (kernelTransformVolume, backprojectionFDK.cu:131-148).
+__global__ void transform_volume_kernel(const float *__restrict__ src, float *__restrict__ dst, int nxs, int nys,
+                                        long long D, long long z_begin, int dz) {
+    __shared__ float tile[32][33];
+    const int x0 = blockIdx.x * 32, z0 = blockIdx.z * 32;
+    const int y = blockIdx.y;
+    // read: consecutive threads walk zs (contiguous in src)
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int x = x0 + r, z = z0 + threadIdx.x;
+        if (x < nxs && z < dz) tile[r][threadIdx.x] = src[((long long)x * nys + y) * D + z_begin + z];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int z = z0 + r, x = x0 + threadIdx.x;
+        if (x < nxs && z < dz) dst[((long long)z * nys + y) * nxs + x] = tile[threadIdx.x][r];
+    }
+}
+
+int transform_volume_to_host(const float *d_vol, int nxs, int nys, long long D, float *host, cudaStream_t st) {
+    // chunk of z slices staged through a bounded device buffer
+    const long long plane = (long long)nxs * nys;
+    long long dz = (256ll << 20) / (plane * 4);
+    if (dz < 1) dz = 1;
+    if (dz > D) dz = D;
+    float *tmp = nullptr;
+    FDK_CUDA(cudaMalloc(&tmp, sizeof(float) * plane * dz));
+    int s = FDK_OK;
+    for (long long z = 0; z < D && s == FDK_OK; z += dz) {
+        const int n = (int)std::min(dz, D - z);
+        const dim3 grid((unsigned)ceil_div(nxs, 32), nys, (unsigned)ceil_div(n, 32));
+        transform_volume_kernel<<<grid, dim3(32, 8), 0, st>>>(d_vol, tmp, nxs, nys, D, z, n);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host + plane * z, tmp, sizeof(float) * plane * n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = cuda_status(e, "GetVolumeData", __FILE__, __LINE__);
+    }
+    cudaFree(tmp);
+    return s;
+}
+
+// TRANSPOSED f32 views (height = nu rows of width = nv) -> MIRROR pairs (u, v) = (v, nv-1-v).
+template <typename T2>
+__global__ void to_mirror_kernel(const float *__restrict__ src, T2 *__restrict__ dst, int width, int height,
+                                 int n) {
+    const long long frame = (long long)width * height;
+    const long long total = frame * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long f = i / frame;
+        const long long r = i - f * frame;
+        const int row = (int)(r / width), v = (int)(r - (long long)row * width);
+        const float *p = src + f * frame + (long long)row * width;
+        const float a = p[v], b = p[width - 1 - v];
+        if constexpr (sizeof(T2) == 8) dst[i] = make_float2(a, b);
+        else dst[i] = __floats2half2_rn(a, b);
+    }
+}
+
+// Largest magnitude of n floats, as the bit pattern of a non-negative float (atomicMax on
+// the unsigned bits orders non-negative floats correctly).
+__global__ void absmax_kernel(const float *__restrict__ x, long long n, unsigned int *out) {
+    float m = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(x[i]));
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+// Power-of-two scale that brings the batch maximum to at most 2^14 in FP16 (exact scaling).
+__device__ __forceinline__ float half_scale(unsigned int absmax_bits) {
+    const float m = fmaxf(__uint_as_float(absmax_bits), 1e-30f);
+    return exp2f(floorf(log2f(16384.f / m)));
+}
+
+// TRANSPOSED f32 views -> MIRROR half2 pairs scaled by half_scale(); acc_scale = 1/scale.
+__global__ void to_mirror_half_kernel(const float *__restrict__ src, __half2 *__restrict__ dst, int width, int height,
+                                      int n, const unsigned int *absmax, float *acc_scale) {
+    const float sc = half_scale(*absmax);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *acc_scale = 1.0f / sc;
+    const long long frame = (long long)width * height;
+    const long long total = frame * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long f = i / frame;
+        const long long r = i - f * frame;
+        const int row = (int)(r / width), v = (int)(r - (long long)row * width);
+        const float *p = src + f * frame + (long long)row * width;
+        dst[i] = __floats2half2_rn(p[v] * sc, p[width - 1 - v] * sc);
+    }
+}
+
+// rows-layout f32 views (nv rows of nu) -> TRANSPOSED f32 (nu rows of nv)
+__global__ void transpose_views_kernel(const float *__restrict__ src, float *__restrict__ dst, int nu, int nv) {
+    __shared__ float tile[32][33];
+    const long long f = blockIdx.z;
+    const float *s = src + f * nu * (long long)nv;
+    float *d = dst + f * nu * (long long)nv;
+    const int u0 = blockIdx.x * 32, v0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int v = v0 + r, u = u0 + threadIdx.x;
+        if (u < nu && v < nv) tile[r][threadIdx.x] = s[(long long)v * nu + u];
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int u = u0 + r, v = v0 + threadIdx.x;
+        if (u < nu && v < nv) d[(long long)u * nv + v] = tile[threadIdx.x][r];
+    }
+}
+
+}  // namespace fdk
+
+using namespace fdk;
+
+struct fdk_bp {
+    int device = 0, precision = FDK_BP_FP32_EXACT;
+    int proj_w = 0, proj_h = 0, proj_count = 0;
+    int nx = 0, ny = 0, nz = 0;
+    fdk_box top{}, bottom{};
+    bool sym = false;
+    long long D = 0;
+    float *d_vol = nullptr;
+    float *d_comp = nullptr;      // compensation term of the MIXED accumulation
+    float *d_stage[2] = {nullptr, nullptr};  // host-view staging (f32, as received)
+    void *d_mirror = nullptr;     // converted views for the fast kernels
+    float *d_mats = nullptr;      // 2 x 128 x 12
+    int slot = 0;
+    cudaStream_t stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr};
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> timers, free_timers;
+    long long bp_count = 0;
+    double kernel_ms = 0;
+    BpFastPlan plan;
+    unsigned int *d_absmax = nullptr;
+    const float *ext_scale = nullptr;  // accumulator scale of FP16 views pushed by the reconstructor
+};
+
+namespace {
+
+int collect_timers(fdk_bp *h) {
+    for (auto &t : h->timers) {
+        FDK_CUDA(cudaEventSynchronize(t.second));
+        float ms = 0;
+        FDK_CUDA(cudaEventElapsedTime(&ms, t.first, t.second));
+        h->kernel_ms += ms;
+        h->free_timers.push_back(t);
+    }
+    h->timers.clear();
+    return FDK_OK;
+}
+
+int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
+    if (h->free_timers.empty()) {
+        if (h->timers.size() >= 64) FDK_TRY(collect_timers(h));
+    }
+    if (!h->free_timers.empty()) {
+        t = h->free_timers.back();
+        h->free_timers.pop_back();
+        return FDK_OK;
+    }
+    FDK_CUDA(cudaEventCreate(&t.first));
+    FDK_CUDA(cudaEventCreate(&t.second));
+    return FDK_OK;
+}
+
+// Backproject n views already resident on the device.
+//   layout TRANSPOSED: f32 frames of proj_h rows x proj_w (the reference's BP input)
+//   layout MIRROR: mirror pairs (f32x2 or f16x2 per precision), proj_h rows x proj_w pairs
+int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const float *d_mats, int n,
+              int width, int height, cudaStream_t st, const float *acc_scale = nullptr) {
+    std::pair<cudaEvent_t, cudaEvent_t> tm;
+    FDK_TRY(take_timer(h, tm));
+    FDK_CUDA(cudaEventRecord(tm.first, st));
+    if (h->precision == FDK_BP_FP32_EXACT) {
+        FDK_CHECK_ARG(layout == FDK_LAYOUT_TRANSPOSED || layout == FDK_LAYOUT_ROWS,
+                      "FP32_EXACT reads f32 frames (TRANSPOSED or ROWS layout)");
+        BpExactArgs a;
+        a.vol = h->d_vol;
+        a.proj = (const float *)dev_proj;
+        a.mats = d_mats;
+        a.width = width;
+        a.height = height;
+        a.n_proj = n;
+        a.x0 = (int)h->top.x;
+        a.y0 = (int)h->top.y;
+        a.z0 = (int)h->top.z;
+        a.nxs = (int)h->top.width;
+        a.nys = (int)h->top.height;
+        a.nzz = h->sym ? (int)(h->D / 2) : (int)h->top.depth;
+        a.D = h->D;
+        a.transpose = transpose;
+        const dim3 grid((unsigned)ceil_div(a.nzz, 32), (unsigned)ceil_div(a.nys, 8), a.nxs);
+        if (h->sym && transpose) bp_exact_kernel<true, true><<<grid, dim3(32, 8), 0, st>>>(a);
+        else if (h->sym) bp_exact_kernel<true, false><<<grid, dim3(32, 8), 0, st>>>(a);
+        else if (transpose) bp_exact_kernel<false, true><<<grid, dim3(32, 8), 0, st>>>(a);
+        else bp_exact_kernel<false, false><<<grid, dim3(32, 8), 0, st>>>(a);
+        FDK_CUDA(cudaGetLastError());
+    } else {
+        FDK_CHECK_ARG(layout == FDK_LAYOUT_MIRROR, "fast backprojection reads the MIRROR layout");
+        FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, 1.0e6f, acc_scale));
+    }
+    FDK_CUDA(cudaEventRecord(tm.second, st));
+    h->timers.push_back(tm);
+    h->bp_count += n;
+    return FDK_OK;
+}
+
+// The fast kernels need circular-orbit matrices: rows 0 and 2 without a z term.
+int check_circular(const float *mats, int n) {
+    for (int i = 0; i < n; i++)
+        FDK_CHECK_ARG(mats[12 * i + 2] == 0.0f && mats[12 * i + 10] == 0.0f,
+                      "view %d: matrix rows 0/2 have a z term; the staged kernels need a circular orbit "
+                      "(use FDK_BP_FP32_EXACT or the RTK entry point)", i);
+    return FDK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t proj_count, int32_t nx, int32_t ny,
+                  int32_t nz, const fdk_box *sub_top, const fdk_box *sub_bottom, int32_t precision, int32_t device) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(out && sub_top && sub_bottom, "NULL argument");
+    *out = nullptr;
+    FDK_CHECK_ARG(proj_width > 1 && proj_height > 1 && proj_count > 0 && proj_count <= 128,
+                  "projection size/count out of range (count <= 128)");
+    FDK_CHECK_ARG(nx > 0 && ny > 0 && nz > 0, "volume size must be positive");
+    FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
+    const fdk_box t = *sub_top, b = *sub_bottom;
+    FDK_CHECK_ARG(t.width > 0 && t.height > 0 && t.depth > 0, "empty top box");
+    FDK_CHECK_ARG(t.x + t.width <= (uint64_t)nx && t.y + t.height <= (uint64_t)ny && t.z + t.depth <= (uint64_t)nz,
+                  "top box outside the volume");
+    const bool sym = b.depth > 0;
+    if (sym) {
+        // mirror-symmetric slab pair (backprojectionFDK.cu:171-173)
+        FDK_CHECK_ARG(t.z + b.z + b.depth - 1 == (uint64_t)nz - 1, "subTop.MinZ + subBottom.MaxZ != nz - 1");
+        FDK_CHECK_ARG(b.depth == t.depth, "mirror slabs must have equal depth");
+        FDK_CHECK_ARG(b.x == t.x && b.y == t.y && b.width == t.width && b.height == t.height,
+                      "mirror slabs must share their x/y extent");
+    }
+    DeviceGuard dg(device);
+    FDK_TRY(dg.status);
+    fdk_bp *h = new fdk_bp();
+    h->device = device;
+    h->precision = precision;
+    h->proj_w = proj_width;
+    h->proj_h = proj_height;
+    h->proj_count = proj_count;
+    h->nx = nx;
+    h->ny = ny;
+    h->nz = nz;
+    h->top = t;
+    h->bottom = b;
+    h->sym = sym;
+    h->D = (long long)t.depth + (sym ? b.depth : 0);
+    const size_t nvox = (size_t)t.width * t.height * h->D;
+    const size_t frame = (size_t)proj_width * proj_height;
+    int s = FDK_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
+    };
+    ck(cudaMalloc(&h->d_vol, sizeof(float) * nvox), "volume");
+    if (s == FDK_OK) ck(cudaMemset(h->d_vol, 0, sizeof(float) * nvox), "volume zero");
+    for (int i = 0; i < 2 && s == FDK_OK; i++) {
+        ck(cudaMalloc(&h->d_stage[i], sizeof(float) * frame * proj_count), "view staging");
+        ck(cudaEventCreateWithFlags(&h->copied[i], cudaEventDisableTiming), "event");
+        ck(cudaEventCreateWithFlags(&h->consumed[i], cudaEventDisableTiming), "event");
+    }
+    if (s == FDK_OK) ck(cudaMalloc(&h->d_mats, sizeof(float) * 2 * 128 * 12), "matrices");
+    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+    if (s == FDK_OK && precision != FDK_BP_FP32_EXACT) {
+        const size_t esz = precision == FDK_BP_MIXED ? sizeof(__half2) : sizeof(float2);
+        ck(cudaMalloc(&h->d_mirror, esz * frame * proj_count), "mirror staging");
+        if (s == FDK_OK && precision == FDK_BP_MIXED) {
+            ck(cudaMalloc(&h->d_absmax, sizeof(unsigned int)), "absmax");
+            ck(cudaMalloc(&h->d_comp, sizeof(float) * nvox), "compensation");
+            if (s == FDK_OK) ck(cudaMemset(h->d_comp, 0, sizeof(float) * nvox), "compensation zero");
+        }
+        if (s == FDK_OK) {
+            FDK_CHECK_ARG(sym, "the fast backprojection kernels need the mirror slab pair (subBottom.depth > 0)");
+            s = bp_fast_plan(h->plan, precision, proj_width, proj_height, (int)t.x, (int)t.y, (int)t.z,
+                             (int)t.width, (int)t.height, (int)t.depth, h->D, device);
+        }
+    }
+    if (s != FDK_OK) {
+        fdk_bp_destroy(h);
+        return s;
+    }
+    *out = h;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t width, int32_t height,
+              const float *proj_mat, int32_t n_proj) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_proj && proj_mat, "NULL argument");
+    FDK_CHECK_ARG(n_proj > 0 && n_proj <= h->proj_count, "n_proj %d outside 1..%d", n_proj, h->proj_count);
+    FDK_CHECK_ARG((long long)width * height <= (long long)h->proj_w * h->proj_h && width > 1 && height > 1,
+                  "view %dx%d larger than the handle's %dx%d", width, height, h->proj_w, h->proj_h);
+    if (h->precision != FDK_BP_FP32_EXACT) {
+        FDK_CHECK_ARG(transpose == 1 && width == h->proj_w && height == h->proj_h,
+                      "fast precisions take the handle's transposed view size");
+        FDK_TRY(check_circular(proj_mat, n_proj));
+    }
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const int k = h->slot;
+    h->slot ^= 1;
+    const size_t frame = (size_t)width * height;
+    // staging slot k is free once the kernel that last read it has finished
+    FDK_CUDA(cudaStreamWaitEvent(h->copy_stream, h->consumed[k], 0));
+    FDK_CUDA(cudaMemcpyAsync(h->d_stage[k], host_proj, sizeof(float) * frame * n_proj, cudaMemcpyHostToDevice,
+                             h->copy_stream));
+    float *d_mats = h->d_mats + k * 128 * 12;
+    FDK_CUDA(cudaMemcpyAsync(d_mats, proj_mat, sizeof(float) * 12 * n_proj, cudaMemcpyHostToDevice, h->copy_stream));
+    FDK_CUDA(cudaEventRecord(h->copied[k], h->copy_stream));
+    // The caller may reuse host_proj on return: wait for the copy (not for the kernel).
+    FDK_CUDA(cudaEventSynchronize(h->copied[k]));
+    FDK_CUDA(cudaStreamWaitEvent(h->stream, h->copied[k], 0));
+    if (h->precision == FDK_BP_FP32_EXACT) {
+        FDK_TRY(launch_bp(h, h->d_stage[k], transpose ? FDK_LAYOUT_TRANSPOSED : FDK_LAYOUT_ROWS, transpose, d_mats,
+                          n_proj, width, height, h->stream));
+    } else {
+        const long long total = (long long)frame * n_proj;
+        const int blocks = (int)std::min<long long>(ceil_div(total, 256), 148 * 16);
+        const float *acc_scale = nullptr;
+        if (h->precision == FDK_BP_MIXED) {
+            FDK_CUDA(cudaMemsetAsync(h->d_absmax, 0, sizeof(unsigned int), h->stream));
+            absmax_kernel<<<blocks, 256, 0, h->stream>>>(h->d_stage[k], total, h->d_absmax);
+            to_mirror_half_kernel<<<blocks, 256, 0, h->stream>>>(h->d_stage[k], (__half2 *)h->d_mirror, width, height,
+                                                                 n_proj, h->d_absmax, h->plan.d_scale);
+            acc_scale = h->plan.d_scale;
+        } else {
+            to_mirror_kernel<float2><<<blocks, 256, 0, h->stream>>>(h->d_stage[k], (float2 *)h->d_mirror, width,
+                                                                    height, n_proj);
+        }
+        FDK_CUDA(cudaGetLastError());
+        FDK_TRY(launch_bp(h, h->d_mirror, FDK_LAYOUT_MIRROR, 1, d_mats, n_proj, width, height, h->stream,
+                          acc_scale));
+    }
+    FDK_CUDA(cudaEventRecord(h->consumed[k], h->stream));
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_bp_device(fdk_bp *h, const void *dev_proj, int32_t layout, const float *proj_mat, int32_t n_proj,
+                     void *stream) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && dev_proj && proj_mat, "NULL argument");
+    FDK_CHECK_ARG(n_proj > 0 && n_proj <= 128, "n_proj %d outside 1..128", n_proj);
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (h->precision != FDK_BP_FP32_EXACT) FDK_TRY(check_circular(proj_mat, n_proj));
+    const int k = h->slot;
+    h->slot ^= 1;
+    float *d_mats = h->d_mats + k * 128 * 12;
+    FDK_CUDA(cudaStreamWaitEvent(st, h->consumed[k], 0));
+    FDK_CUDA(cudaMemcpyAsync(d_mats, proj_mat, sizeof(float) * 12 * n_proj, cudaMemcpyHostToDevice, st));
+    // the matrices come from pageable host memory: the async copy completes before returning
+    FDK_TRY(launch_bp(h, dev_proj, layout, 1, d_mats, n_proj, h->proj_w, h->proj_h, st,
+                      h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr));
+    FDK_CUDA(cudaEventRecord(h->consumed[k], st));
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_get_volume(fdk_bp *h, float *host_vol, int64_t size) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_vol, "NULL argument");
+    const long long nvox = (long long)h->top.width * h->top.height * h->D;
+    FDK_CHECK_ARG(size >= nvox, "size %lld < %lld voxels", (long long)size, nvox);
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_CUDA(cudaStreamSynchronize(h->copy_stream));
+    FDK_CUDA(cudaStreamSynchronize(h->stream));
+    FDK_CUDA(cudaDeviceSynchronize());  // device-resident launches may use caller streams
+    if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
+    return transform_volume_to_host(h->d_vol, (int)h->top.width, (int)h->top.height, h->D, host_vol, h->stream);
+    FDK_ABI_END
+}
+
+int fdk_bp_volume_device(fdk_bp *h, float **dev_vol, int64_t *count) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h && dev_vol && count, "NULL argument");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_CUDA(cudaDeviceSynchronize());
+    const long long nvox = (long long)h->top.width * h->top.height * h->D;
+    if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
+    FDK_CUDA(cudaStreamSynchronize(h->stream));
+    *dev_vol = h->d_vol;
+    *count = nvox;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_stats(fdk_bp *h, int64_t *bp_count, double *kernel_ms) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(collect_timers(h));
+    if (bp_count) *bp_count = h->bp_count;
+    if (kernel_ms) *kernel_ms = h->kernel_ms;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_reset(fdk_bp *h) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_CUDA(cudaDeviceSynchronize());
+    const size_t nvox = (size_t)h->top.width * h->top.height * h->D;
+    FDK_CUDA(cudaMemset(h->d_vol, 0, sizeof(float) * nvox));
+    if (h->d_comp) FDK_CUDA(cudaMemset(h->d_comp, 0, sizeof(float) * nvox));
+    FDK_TRY(collect_timers(h));
+    h->bp_count = 0;
+    h->kernel_ms = 0;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_destroy(fdk_bp *h) {
+    if (!h) return FDK_OK;
+    {
+        DeviceGuard dg(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
+        for (auto &t : h->timers) {
+            cudaEventDestroy(t.first);
+            cudaEventDestroy(t.second);
+        }
+        for (auto &t : h->free_timers) {
+            cudaEventDestroy(t.first);
+            cudaEventDestroy(t.second);
+        }
+        for (int i = 0; i < 2; i++) {
+            if (h->d_stage[i]) cudaFree(h->d_stage[i]);
+            if (h->copied[i]) cudaEventDestroy(h->copied[i]);
+            if (h->consumed[i]) cudaEventDestroy(h->consumed[i]);
+        }
+        if (h->d_mirror) cudaFree(h->d_mirror);
+        if (h->d_vol) cudaFree(h->d_vol);
+        if (h->d_comp) cudaFree(h->d_comp);
+        if (h->d_mats) cudaFree(h->d_mats);
+        if (h->d_absmax) cudaFree(h->d_absmax);
+        bp_fast_release(h->plan);
+        if (h->stream) cudaStreamDestroy(h->stream);
+        if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+    }
+    delete h;
+    return FDK_OK;
+}
+
+}  // extern "C"
+
+// Device scalar multiplying the MIXED accumulators of device-resident FP16 views (their
+// producer divided the filtered values by it).  Internal to the library (recon.cu).
+int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale) {
+    if (!h) return FDK_ERR_INVALID_ARG;
+    h->ext_scale = d_scale;
+    return FDK_OK;
+}

@@ -1,0 +1,424 @@
+// filter.cu -- fused FDK row filter for sm_100a: cosine pre-weight, constant edge pad,
+// ramp/window filter by FFT, crop, and the store in the layout the backprojection reads.
+//
+// Reference semantics: FilterEngine::Filtering (Filterlib/FilterLib.h:167-196) and the cuFFT
+// plugin (FilterlibCufft/cudaFftFilter.cu:14-61, 283-392).  One CTA filters two detector rows
+// at once -- row r and its mirror row nv-1-r -- as the real and imaginary parts of one complex
+// FFT of length W: with a real, even response H the two filtered rows come back as the real
+// and imaginary parts of the inverse transform.  Pairing r with nv-1-r is what lets the same
+// CTA emit the backprojection's mirror-pair layout directly.
+//
+// FFT: radix-2 decimation in frequency (natural -> bit-reversed order), pointwise multiply by
+// H[bitrev(p)]/W, radix-2 decimation in time (bit-reversed -> natural), all in shared memory.
+// Twiddles come from an FP64-computed table.
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.h"
+#include "internal.h"
+
+namespace fdk {
+
+struct FilterArgs {
+    const float *src;   // views of nv rows x nu, row pitch src_pitch, view stride src_vstride
+    void *dst;          // output, layout dependent
+    const float *cos;   // nv x nu (pitch cos_pitch) or nullptr
+    const float2 *tw;   // W/2 twiddles exp(-2 pi i k / W)
+    const float *hb;    // W: H[bitrev(p)] / W
+    int nu, nv, W, log2W, off, pad_n;
+    int src_pitch, dst_pitch, cos_pitch;
+    long long src_vstride, dst_vstride;
+    float out_scale;          // multiplies every output sample (FP16 range control)
+    unsigned int *overflow;   // set to 1 when a scaled FP16 output exceeds the format (or NULL)
+};
+
+template <typename OUT>
+__device__ __forceinline__ OUT to_out(const FilterArgs &a, float y) {
+    if constexpr (sizeof(OUT) == 2) {
+        const float s = y * a.out_scale;
+        if (a.overflow && !(fabsf(s) <= 65504.f)) atomicOr(a.overflow, 1u);
+        return __float2half_rn(s);
+    } else {
+        return y * a.out_scale;
+    }
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// Weighted sample of row r at column c of the current view.
+__device__ __forceinline__ float row_sample(const FilterArgs &a, const float *view, int r, int c) {
+    float x = __ldg(view + (long long)r * a.src_pitch + c);
+    if (a.cos) x *= __ldg(a.cos + (long long)r * a.cos_pitch + c);
+    return x;
+}
+
+// Mean of the first (or last) pad_n weighted samples of row r.
+__device__ float edge_mean(const FilterArgs &a, const float *view, int r, bool left) {
+    float s = 0.f;
+    for (int k = 0; k < a.pad_n; k++) s += row_sample(a, view, r, left ? k : a.nu - 1 - k);
+    return s / (float)a.pad_n;
+}
+
+// LAYOUT: FDK_LAYOUT_ROWS, FDK_LAYOUT_TRANSPOSED, FDK_LAYOUT_MIRROR; OUT: float or __half
+template <int LAYOUT, typename OUT>
+__global__ void __launch_bounds__(256) filter_rows_kernel(FilterArgs a) {
+    extern __shared__ float2 buf[];
+    __shared__ float pads[4];
+    const int r1 = blockIdx.x;
+    const int r2 = a.nv - 1 - r1;
+    const int view = blockIdx.y;
+    const float *vsrc = a.src + (long long)view * a.src_vstride;
+    const int W = a.W;
+
+    if (threadIdx.x < 4) {
+        const int r = (threadIdx.x < 2) ? r1 : r2;
+        pads[threadIdx.x] = edge_mean(a, vsrc, r, (threadIdx.x & 1) == 0);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < W; k += blockDim.x) {
+        const int c = k - a.off;
+        float x1, x2;
+        if (c < 0) {
+            x1 = pads[0]; x2 = pads[2];
+        } else if (c >= a.nu) {
+            x1 = pads[1]; x2 = pads[3];
+        } else {
+            x1 = row_sample(a, vsrc, r1, c);
+            x2 = row_sample(a, vsrc, r2, c);
+        }
+        buf[k] = make_float2(x1, x2);
+    }
+    __syncthreads();
+
+    // forward: decimation in frequency
+    for (int half = W >> 1, step = 1; half >= 1; half >>= 1, step <<= 1) {
+        for (int b = threadIdx.x; b < (W >> 1); b += blockDim.x) {
+            const int j = b & (half - 1);
+            const int i0 = ((b - j) << 1) + j;
+            const int i1 = i0 + half;
+            const float2 x = buf[i0], y = buf[i1];
+            buf[i0] = make_float2(x.x + y.x, x.y + y.y);
+            buf[i1] = cmul(make_float2(x.x - y.x, x.y - y.y), __ldg(a.tw + j * step));
+        }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < W; k += blockDim.x) {
+        const float h = __ldg(a.hb + k);
+        float2 v = buf[k];
+        buf[k] = make_float2(v.x * h, v.y * h);
+    }
+    __syncthreads();
+    // inverse: decimation in time, conjugate twiddles
+    for (int half = 1, step = W >> 1; half < W; half <<= 1, step >>= 1) {
+        for (int b = threadIdx.x; b < (W >> 1); b += blockDim.x) {
+            const int j = b & (half - 1);
+            const int i0 = ((b - j) << 1) + j;
+            const int i1 = i0 + half;
+            const float2 x = buf[i0];
+            const float2 t = cmulc(buf[i1], __ldg(a.tw + j * step));
+            buf[i0] = make_float2(x.x + t.x, x.y + t.y);
+            buf[i1] = make_float2(x.x - t.x, x.y - t.y);
+        }
+        __syncthreads();
+    }
+
+    OUT *dst = reinterpret_cast<OUT *>(a.dst);
+    for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
+        const float2 y = buf[a.off + u];
+        const OUT o1 = to_out<OUT>(a, y.x), o2 = to_out<OUT>(a, y.y);
+        if (LAYOUT == FDK_LAYOUT_ROWS) {
+            OUT *d = dst + (long long)view * a.dst_vstride;
+            d[(long long)r1 * a.dst_pitch + u] = o1;
+            if (r2 != r1) d[(long long)r2 * a.dst_pitch + u] = o2;
+        } else if (LAYOUT == FDK_LAYOUT_TRANSPOSED) {
+            OUT *d = dst + (long long)view * a.dst_vstride + (long long)u * a.dst_pitch;
+            d[r1] = o1;
+            if (r2 != r1) d[r2] = o2;
+        } else {  // mirror pairs: element (u, v) = (row v, row nv-1-v)
+            OUT *d = dst + (long long)view * a.dst_vstride + (long long)u * a.dst_pitch * 2;
+            d[2 * r1] = o1;
+            d[2 * r1 + 1] = o2;
+            if (r2 != r1) {
+                d[2 * r2] = o2;
+                d[2 * r2 + 1] = o1;
+            }
+        }
+    }
+}
+
+int FilterTables::create(const double *H, int W_) {
+    W = W_;
+    log2W = 0;
+    while ((1 << log2W) < W) log2W++;
+    std::vector<float2> t(W / 2);
+    for (int k = 0; k < W / 2; k++) {
+        const double ang = -2.0 * 3.14159265358979323846 * k / W;
+        t[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+    }
+    std::vector<float> h(W);
+    for (int p = 0; p < W; p++) {
+        int r = 0;
+        for (int b = 0; b < log2W; b++)
+            if (p & (1 << b)) r |= 1 << (log2W - 1 - b);
+        h[p] = (float)(H[r] / W);
+    }
+    FDK_CUDA(cudaMalloc(&tw, sizeof(float2) * (W / 2)));
+    FDK_CUDA(cudaMalloc(&hb, sizeof(float) * W));
+    FDK_CUDA(cudaMemcpy(tw, t.data(), sizeof(float2) * (W / 2), cudaMemcpyHostToDevice));
+    FDK_CUDA(cudaMemcpy(hb, h.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
+    return FDK_OK;
+}
+
+void FilterTables::release() {
+    if (tw) cudaFree(tw);
+    if (hb) cudaFree(hb);
+    tw = nullptr;
+    hb = nullptr;
+}
+
+static int launch_filter(const FilterArgs &a, int n_views, int layout, int dtype, cudaStream_t st) {
+    const dim3 grid((a.nv + 1) / 2, n_views);
+    const size_t smem = sizeof(float2) * a.W;
+    if (smem > 48 * 1024) {
+        // opt in to more than 48 KB of dynamic shared memory for every instantiation used
+        static bool done = false;
+        if (!done) {
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+            done = true;
+        }
+    }
+#define FDK_LAUNCH(L, T) filter_rows_kernel<L, T><<<grid, 256, smem, st>>>(a)
+    if (dtype == FDK_DTYPE_F32) {
+        if (layout == FDK_LAYOUT_ROWS) FDK_LAUNCH(FDK_LAYOUT_ROWS, float);
+        else if (layout == FDK_LAYOUT_TRANSPOSED) FDK_LAUNCH(FDK_LAYOUT_TRANSPOSED, float);
+        else FDK_LAUNCH(FDK_LAYOUT_MIRROR, float);
+    } else {
+        if (layout == FDK_LAYOUT_ROWS) FDK_LAUNCH(FDK_LAYOUT_ROWS, __half);
+        else if (layout == FDK_LAYOUT_TRANSPOSED) FDK_LAUNCH(FDK_LAYOUT_TRANSPOSED, __half);
+        else FDK_LAUNCH(FDK_LAYOUT_MIRROR, __half);
+    }
+#undef FDK_LAUNCH
+    FDK_CUDA(cudaGetLastError());
+    return FDK_OK;
+}
+
+// Shared by the FilterEngine handle, the cuFFT-plugin entry points and the reconstructor.
+int filter_views(const float *src, int src_pitch, long long src_vstride, void *dst, int dst_pitch,
+                 long long dst_vstride, const float *cos, int cos_pitch, const FilterTables &t, int nu,
+                 int nv, int pad_n, int n_views, int layout, int dtype, cudaStream_t st, float out_scale,
+                 unsigned int *overflow) {
+    FilterArgs a;
+    a.src = src;
+    a.dst = dst;
+    a.cos = cos;
+    a.tw = t.tw;
+    a.hb = t.hb;
+    a.nu = nu;
+    a.nv = nv;
+    a.W = t.W;
+    a.log2W = t.log2W;
+    a.off = (t.W - nu) >> 1;
+    a.pad_n = pad_n;
+    a.src_pitch = src_pitch;
+    a.dst_pitch = dst_pitch;
+    a.cos_pitch = cos_pitch;
+    a.src_vstride = src_vstride;
+    a.dst_vstride = dst_vstride;
+    a.out_scale = out_scale;
+    a.overflow = overflow;
+    return launch_filter(a, n_views, layout, dtype, st);
+}
+
+static int check_filter_dims(int64_t nu, int64_t nv, int64_t W, int pad) {
+    FDK_CHECK_ARG(nu > 0 && nv > 0, "nu, nv must be positive");
+    FDK_CHECK_ARG(W >= nu && W <= 4096 && (W & (W - 1)) == 0, "W=%lld must be a power of two in [nu, 4096]",
+                  (long long)W);
+    FDK_CHECK_ARG(pad >= 1 && pad <= 4 && pad <= nu, "pad_edge must be 1..4 and <= nu");
+    FDK_CHECK_ARG(nv <= 65535 * 2, "nv too large");
+    return FDK_OK;
+}
+
+// Kernel dst = src * table (kernelCorrect, cudaFftFilter.cu:270-281).
+__global__ void correct_kernel(const float *src, float *dst, int pitch, int width, int height, int depth,
+                               const float *table, int tpitch) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    const int z = blockIdx.z;
+    if (x >= width || y >= height || z >= depth) return;
+    const long long o = ((long long)z * height + y) * pitch + x;
+    dst[o] = src[o] * table[(long long)y * tpitch + x];
+}
+
+}  // namespace fdk
+
+struct fdk_filter {
+    int device = 0;
+    int64_t nu = 0, nv = 0, W = 0;
+    int pad = 4;
+    float *d_cos = nullptr;
+    float *d_src = nullptr;
+    float *d_dst = nullptr;
+    fdk::FilterTables tables;
+    cudaStream_t stream = nullptr;
+};
+
+using namespace fdk;
+
+extern "C" {
+
+int fdk_filter_create(fdk_filter **out, const float *cos_table, const float *H, int64_t nu, int64_t nv,
+                      int64_t W, int32_t pad_edge, int32_t device) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(out != nullptr && H != nullptr, "out or H is NULL");
+    *out = nullptr;
+    FDK_TRY(check_filter_dims(nu, nv, W, pad_edge));
+    DeviceGuard dg(device);
+    FDK_TRY(dg.status);
+    fdk_filter *h = new fdk_filter();
+    h->device = device;
+    h->nu = nu;
+    h->nv = nv;
+    h->W = W;
+    h->pad = pad_edge;
+    std::vector<double> Hd(H, H + W);
+    int s = h->tables.create(Hd.data(), (int)W);
+    if (s == FDK_OK && cos_table) {
+        cudaError_t e = cudaMalloc(&h->d_cos, sizeof(float) * nu * nv);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_cos, cos_table, sizeof(float) * nu * nv, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) s = cuda_status(e, "filter cos table", __FILE__, __LINE__);
+    }
+    if (s == FDK_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) s = cuda_status(e, "cudaStreamCreate", __FILE__, __LINE__);
+    }
+    if (s != FDK_OK) {
+        fdk_filter_destroy(h);
+        return s;
+    }
+    *out = h;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_filter_filtering(fdk_filter *h, float *src_host, float *dst_host, int32_t transpose) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && src_host && dst_host, "NULL argument");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const size_t n = (size_t)h->nu * h->nv;
+    // FilterCosCorrect (FilterLib.h:8-13): src *= cos, in place on the caller's buffer, in FP32.
+    if (h->d_cos) {
+        std::vector<float> cos(n);
+        FDK_CUDA(cudaMemcpy(cos.data(), h->d_cos, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; i++) src_host[i] = src_host[i] * cos[i];
+    }
+    if (!h->d_src) {
+        FDK_CUDA(cudaMalloc(&h->d_src, sizeof(float) * n));
+        FDK_CUDA(cudaMalloc(&h->d_dst, sizeof(float) * n));
+    }
+    FDK_CUDA(cudaMemcpyAsync(h->d_src, src_host, sizeof(float) * n, cudaMemcpyHostToDevice, h->stream));
+    const int layout = transpose ? FDK_LAYOUT_TRANSPOSED : FDK_LAYOUT_ROWS;
+    const int dpitch = transpose ? (int)h->nv : (int)h->nu;
+    FDK_TRY(filter_views(h->d_src, (int)h->nu, (long long)n, h->d_dst, dpitch, (long long)n, nullptr, 0,
+                         h->tables, (int)h->nu, (int)h->nv, h->pad, 1, layout, FDK_DTYPE_F32, h->stream));
+    FDK_CUDA(cudaMemcpyAsync(dst_host, h->d_dst, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    FDK_CUDA(cudaStreamSynchronize(h->stream));
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, int64_t n_views, int32_t layout,
+                          int32_t out_dtype, void *stream) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && src_dev && dst_dev, "NULL argument");
+    FDK_CHECK_ARG(n_views > 0 && n_views <= 65535, "n_views out of range");
+    FDK_CHECK_ARG(layout >= FDK_LAYOUT_ROWS && layout <= FDK_LAYOUT_MIRROR, "bad layout");
+    FDK_CHECK_ARG(out_dtype == FDK_DTYPE_F32 || out_dtype == FDK_DTYPE_F16, "bad dtype");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const long long n = (long long)h->nu * h->nv;
+    const int dpitch = layout == FDK_LAYOUT_ROWS ? (int)h->nu : (int)h->nv;
+    const long long dstride = layout == FDK_LAYOUT_MIRROR ? 2 * n : n;
+    return filter_views(src_dev, (int)h->nu, n, dst_dev, dpitch, dstride, h->d_cos, (int)h->nu, h->tables,
+                        (int)h->nu, (int)h->nv, h->pad, (int)n_views, layout, out_dtype,
+                        (cudaStream_t)stream);
+    FDK_ABI_END
+}
+
+int fdk_filter_destroy(fdk_filter *h) {
+    if (!h) return FDK_OK;
+    {
+        DeviceGuard dg(h->device);
+        if (h->stream) cudaStreamSynchronize(h->stream);
+        h->tables.release();
+        if (h->d_cos) cudaFree(h->d_cos);
+        if (h->d_src) cudaFree(h->d_src);
+        if (h->d_dst) cudaFree(h->d_dst);
+        if (h->stream) cudaStreamDestroy(h->stream);
+    }
+    delete h;
+    return FDK_OK;
+}
+
+int fdk_correct_image_real32(const fdk_dataref *src, const fdk_dataref *table, fdk_dataref *dst) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(src && table && dst && src->data && table->data && dst->data, "NULL argument");
+    FDK_CHECK_ARG(src->pitch == dst->pitch && src->width == dst->width && src->height == dst->height &&
+                      src->depth <= dst->depth,
+                  "src/dst shapes differ (CorrectImage, cudaFftFilter.cu:286-289)");
+    FDK_CHECK_ARG(src->width > 0 && src->height > 0 && src->depth > 0 && src->pitch >= src->width, "bad shape");
+    FDK_CHECK_ARG(src->height <= 65535 && src->depth <= 65535, "shape too large");
+    const dim3 grid((unsigned)ceil_div(src->width, 128), src->height, src->depth);
+    correct_kernel<<<grid, 128>>>(src->data, dst->data, src->pitch, src->width, src->height, src->depth,
+                                  table->data, table->pitch);
+    FDK_CUDA(cudaGetLastError());
+    FDK_CUDA(cudaDeviceSynchronize());
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_filter_row_real32(const fdk_dataref *src, fdk_dataref *dst, const fdk_dataref *filter) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(src && dst && filter && src->data && dst->data && filter->data, "NULL argument");
+    FDK_CHECK_ARG(src->width == dst->width && src->height == dst->height && src->depth <= dst->depth,
+                  "src/dst shapes differ (FilterRow, cudaFftFilter.cu:302-305)");
+    FDK_CHECK_ARG(filter->height == 1 || filter->height == 0, "filter must be one row");
+    const int W = filter->width;
+    FDK_TRY(check_filter_dims(src->width, src->height, W, 3));
+    std::vector<float> Hf(W);
+    FDK_CUDA(cudaMemcpy(Hf.data(), filter->data, sizeof(float) * W, cudaMemcpyDeviceToHost));
+    std::vector<double> Hd(Hf.begin(), Hf.end());
+    FilterTables t;
+    int s = t.create(Hd.data(), W);
+    if (s == FDK_OK)
+        s = filter_views(src->data, src->pitch, (long long)src->pitch * src->height, dst->data, dst->pitch,
+                         (long long)dst->pitch * dst->height, nullptr, 0, t, src->width, src->height, 3,
+                         src->depth, FDK_LAYOUT_ROWS, FDK_DTYPE_F32, 0);
+    if (s == FDK_OK) {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) s = cuda_status(e, "FilterRow sync", __FILE__, __LINE__);
+    }
+    t.release();
+    return s;
+    FDK_ABI_END
+}
+
+}  // extern "C"

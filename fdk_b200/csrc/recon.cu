@@ -1,0 +1,306 @@
+// recon.cu -- end-to-end streaming FDK on one GPU: the single-GPU analogue of cuFDK's
+// FilterThread -> BpThread handoff (cuFDK/mpiFDK.cpp:58-317).
+//
+//   host views --(copy stream, 2 staging slots)--> raw views on the device
+//   --(compute stream)--> fused cosine weight + ramp filter, written straight into the
+//   backprojection's layout --> backprojection into the resident volume.
+//
+// The whole volume is one mirror-symmetric slab pair (DivVolume with one rank,
+// cuFDK/mpiFDK.h:116-149): top = z in [0, nz/2), bottom = z in [nz/2, nz).  Host waits are
+// bounded: fdk_recon_sync polls with a deadline and returns FDK_ERR_TIMEOUT instead of hanging.
+#include <cuda_fp16.h>
+
+#include <chrono>
+#include <thread>
+#include <vector>
+
+#include "common.h"
+#include "internal.h"
+
+using namespace fdk;
+
+struct fdk_recon {
+    fdk_geometry g{};
+    int precision = FDK_BP_FP32;
+    int batch = 32;
+    int device = 0;
+    int pad = 4;  // edge pad of the production IPP filter plugin (Filterlib/FilterLib.h:38,44)
+    int layout = FDK_LAYOUT_MIRROR;
+    int dtype = FDK_DTYPE_F32;
+    fdk_bp *bp = nullptr;
+    FilterTables tables;
+    float *d_cos = nullptr;
+    float *d_raw[2] = {nullptr, nullptr};
+    void *d_filt = nullptr;
+    float *d_scale = nullptr;        // accumulator scale of FP16 views (device scalar)
+    unsigned int *d_overflow = nullptr;
+    float out_scale = 1.0f;
+    std::vector<float> mats;         // 12 x n_proj, FP32 (from FP64)
+    cudaStream_t compute = nullptr, copy = nullptr;
+    cudaEvent_t raw_ready[2] = {nullptr, nullptr}, raw_free[2] = {nullptr, nullptr};
+    cudaEvent_t f0 = nullptr, f1 = nullptr, done = nullptr;
+    int slot = 0;
+    double filter_ms = 0;
+    long long views = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
+};
+
+// fast-path accumulator scale hook (bp.cu)
+int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
+
+namespace {
+
+int recon_release(fdk_recon *h) {
+    if (!h) return FDK_OK;
+    DeviceGuard dg(h->device);
+    if (h->compute) cudaStreamSynchronize(h->compute);
+    if (h->copy) cudaStreamSynchronize(h->copy);
+    if (h->bp) fdk_bp_destroy(h->bp);
+    h->tables.release();
+    for (int i = 0; i < 2; i++) {
+        if (h->d_raw[i]) cudaFree(h->d_raw[i]);
+        if (h->raw_ready[i]) cudaEventDestroy(h->raw_ready[i]);
+        if (h->raw_free[i]) cudaEventDestroy(h->raw_free[i]);
+    }
+    for (auto &t : h->ftimers) {
+        cudaEventDestroy(t.first);
+        cudaEventDestroy(t.second);
+    }
+    if (h->d_cos) cudaFree(h->d_cos);
+    if (h->d_filt) cudaFree(h->d_filt);
+    if (h->d_scale) cudaFree(h->d_scale);
+    if (h->d_overflow) cudaFree(h->d_overflow);
+    if (h->done) cudaEventDestroy(h->done);
+    if (h->compute) cudaStreamDestroy(h->compute);
+    if (h->copy) cudaStreamDestroy(h->copy);
+    delete h;
+    return FDK_OK;
+}
+
+int collect_filter_timers(fdk_recon *h) {
+    for (auto &t : h->ftimers) {
+        FDK_CUDA(cudaEventSynchronize(t.second));
+        float ms = 0;
+        FDK_CUDA(cudaEventElapsedTime(&ms, t.first, t.second));
+        h->filter_ms += ms;
+        cudaEventDestroy(t.first);
+        cudaEventDestroy(t.second);
+    }
+    h->ftimers.clear();
+    return FDK_OK;
+}
+
+// Filter + backproject views [first, first+n) whose raw data is at d_src (nv x nu each).
+int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cudaEvent_t release) {
+    const fdk_geometry &g = h->g;
+    const long long frame = g.nu * g.nv;
+    std::pair<cudaEvent_t, cudaEvent_t> t;
+    FDK_CUDA(cudaEventCreate(&t.first));
+    FDK_CUDA(cudaEventCreate(&t.second));
+    FDK_CUDA(cudaEventRecord(t.first, h->compute));
+    const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
+    FDK_TRY(filter_views(d_src, (int)g.nu, frame, h->d_filt, (int)g.nv, dstride, h->d_cos, (int)g.nu, h->tables,
+                         (int)g.nu, (int)g.nv, h->pad, n, h->layout, h->dtype,
+                         h->compute, h->out_scale, h->d_overflow));
+    FDK_CUDA(cudaEventRecord(t.second, h->compute));
+    h->ftimers.push_back(t);
+    if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
+    if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
+    FDK_TRY(fdk_bp_bp_device(h->bp, h->d_filt, h->layout, h->mats.data() + 12 * first, n, h->compute));
+    h->views += n;
+    return FDK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch, int32_t device) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(out && g, "NULL argument");
+    *out = nullptr;
+    FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
+    FDK_CHECK_ARG(batch > 0 && batch <= 128, "batch must be 1..128");
+    FDK_CHECK_ARG(g->nz % 2 == 0, "the slab-pair reconstructor needs an even nz");
+    FDK_CHECK_ARG(g->nx <= 65535 * 16 && g->ny <= 65535 * 16, "volume too large");
+    const int64_t W = fdk_filter_length(g->nu);
+    FDK_CHECK_ARG(W <= 4096, "detector too wide: nextpow2(nu) = %lld > 4096", (long long)W);
+    if (precision == FDK_BP_FP32_EXACT) FDK_CHECK_ARG(batch <= 32, "FP32_EXACT batches are <= 32 views");
+    DeviceGuard dg(device);
+    FDK_TRY(dg.status);
+    fdk_recon *h = new fdk_recon();
+    h->g = *g;
+    h->precision = precision;
+    h->batch = batch;
+    h->device = device;
+    h->layout = precision == FDK_BP_FP32_EXACT ? FDK_LAYOUT_TRANSPOSED : FDK_LAYOUT_MIRROR;
+    h->dtype = precision == FDK_BP_MIXED ? FDK_DTYPE_F16 : FDK_DTYPE_F32;
+    int s = FDK_OK;
+    auto ck = [&](cudaError_t e, const char *what) {
+        if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
+    };
+    // geometry tables (FP64 -> FP32)
+    std::vector<double> H(W);
+    std::vector<float> cos(g->nu * g->nv);
+    h->mats.resize(12 * g->n_proj);
+    s = fdk_filter_design(g->filter_type, g->nu, 1, H.data(), W);
+    if (s == FDK_OK) s = fdk_cos_table(g, cos.data());
+    if (s == FDK_OK) s = fdk_projection_matrices(g, nullptr, h->mats.data());
+    if (s == FDK_OK) s = h->tables.create(H.data(), (int)W);
+    const long long frame = g->nu * g->nv;
+    if (s == FDK_OK) ck(cudaMalloc(&h->d_cos, sizeof(float) * frame), "cos table");
+    if (s == FDK_OK) ck(cudaMemcpy(h->d_cos, cos.data(), sizeof(float) * frame, cudaMemcpyHostToDevice), "cos copy");
+    for (int i = 0; i < 2 && s == FDK_OK; i++) {
+        ck(cudaMalloc(&h->d_raw[i], sizeof(float) * frame * batch), "raw views");
+        ck(cudaEventCreateWithFlags(&h->raw_ready[i], cudaEventDisableTiming), "event");
+        ck(cudaEventCreateWithFlags(&h->raw_free[i], cudaEventDisableTiming), "event");
+    }
+    const size_t esz = h->layout == FDK_LAYOUT_MIRROR ? (h->dtype == FDK_DTYPE_F16 ? 4 : 8) : 4;
+    if (s == FDK_OK) ck(cudaMalloc(&h->d_filt, esz * frame * batch), "filtered views");
+    if (s == FDK_OK) ck(cudaMalloc(&h->d_overflow, sizeof(unsigned int)), "overflow flag");
+    if (s == FDK_OK) ck(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)), "overflow flag");
+    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->compute, cudaStreamNonBlocking), "stream");
+    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "stream");
+    if (s == FDK_OK) ck(cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming), "event");
+    if (s == FDK_OK && h->dtype == FDK_DTYPE_F16) {
+        // FP16 views hold the filtered values divided by the cosine table's SOD^2 * AAF factor
+        // (raw line-integral units); the backprojection multiplies it back.
+        double aaf = 0;
+        s = fdk_angular_ramp_factor(g, &aaf);
+        const float k = (float)(g->sod * g->sod * aaf);
+        h->out_scale = 1.0f / k;
+        if (s == FDK_OK) ck(cudaMalloc(&h->d_scale, sizeof(float)), "scale");
+        if (s == FDK_OK) ck(cudaMemcpy(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice), "scale");
+    }
+    if (s == FDK_OK) {
+        const uint64_t half = g->nz / 2;
+        fdk_box top{0, 0, 0, (uint64_t)g->nx, (uint64_t)g->ny, half};
+        fdk_box bot{0, 0, half, (uint64_t)g->nx, (uint64_t)g->ny, half};
+        s = fdk_bp_create(&h->bp, (int)g->nv, (int)g->nu, precision == FDK_BP_FP32_EXACT ? 32 : batch, (int)g->nx,
+                          (int)g->ny, (int)g->nz, &top, &bot, precision, device);
+        if (s == FDK_OK && h->d_scale) s = fdk_bp_set_acc_scale_internal(h->bp, h->d_scale);
+    }
+    if (s != FDK_OK) {
+        recon_release(h);
+        return s;
+    }
+    *out = h;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t n) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_views, "NULL argument");
+    FDK_CHECK_ARG(first >= 0 && n > 0 && first + n <= h->g.n_proj, "view range [%lld, %lld) outside 0..%lld",
+                  (long long)first, (long long)(first + n), (long long)h->g.n_proj);
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const long long frame = h->g.nu * h->g.nv;
+    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    cudaEvent_t last = nullptr;
+    for (long long c = 0; c < n; c += cap) {
+        const int m = (int)std::min<long long>(cap, n - c);
+        const int k = h->slot;
+        h->slot ^= 1;
+        FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
+        FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], host_views + c * frame, sizeof(float) * frame * m,
+                                 cudaMemcpyHostToDevice, h->copy));
+        FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
+        FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
+        FDK_TRY(process_chunk(h, h->d_raw[k], first + c, m, h->raw_free[k]));
+        last = h->raw_ready[k];
+    }
+    // the caller may reuse host_views once its last copy has landed
+    if (last) FDK_CUDA(cudaEventSynchronize(last));
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && dev_views, "NULL argument");
+    FDK_CHECK_ARG(first >= 0 && n > 0 && first + n <= h->g.n_proj, "view range outside the scan");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const long long frame = h->g.nu * h->g.nv;
+    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    for (long long c = 0; c < n; c += cap) {
+        const int m = (int)std::min<long long>(cap, n - c);
+        FDK_TRY(process_chunk(h, dev_views + c * frame, first + c, m, nullptr));
+    }
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_CUDA(cudaEventRecord(h->done, h->compute));
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t limit = timeout_ms > 0 ? timeout_ms : 600000;
+    for (;;) {
+        cudaError_t e = cudaEventQuery(h->done);
+        if (e == cudaSuccess) break;
+        if (e != cudaErrorNotReady) return cuda_status(e, "fdk_recon_sync", __FILE__, __LINE__);
+        const auto el = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0);
+        if (el.count() > limit) return fail(FDK_ERR_TIMEOUT, "fdk_recon_sync: work not finished after %lld ms",
+                                            (long long)limit);
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    unsigned int ovf = 0;
+    FDK_CUDA(cudaMemcpy(&ovf, h->d_overflow, sizeof(ovf), cudaMemcpyDeviceToHost));
+    if (ovf)
+        return fail(FDK_ERR_DEVICE_CHECK, "filtered views exceeded the FP16 range; use FDK_BP_FP32 for this data");
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_vol, "NULL argument");
+    FDK_TRY(fdk_recon_sync(h, 0));
+    return fdk_bp_get_volume(h->bp, host_vol, size);
+    FDK_ABI_END
+}
+
+int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(collect_filter_timers(h));
+    int64_t cnt = 0;
+    double ms = 0;
+    FDK_TRY(fdk_bp_stats(h->bp, &cnt, &ms));
+    if (bp_ms) *bp_ms = ms;
+    if (filter_ms) *filter_ms = h->filter_ms;
+    if (views) *views = h->views;
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_reset(fdk_recon *h) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_CUDA(cudaStreamSynchronize(h->copy));
+    FDK_CUDA(cudaStreamSynchronize(h->compute));
+    FDK_TRY(collect_filter_timers(h));
+    FDK_CUDA(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)));
+    h->filter_ms = 0;
+    h->views = 0;
+    return fdk_bp_reset(h->bp);
+    FDK_ABI_END
+}
+
+int fdk_recon_destroy(fdk_recon *h) { return recon_release(h); }
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// rtk.cu -- the RTK-style backprojection drop-in, CUDA_reconstruct_conebeam
+// (cudaBP/rtkCudaFDKBackProjectionImageFilter.cu:200-330, kernel_fdk_3Dgrid :156-191,
+// RtkSUBPIXEL :83-112).
+//
+// General 3x4 geometry: every voxel evaluates the full matrix product for every view (no
+// circular-orbit shortcut), so tilted or non-circular trajectories are handled.  Views are
+// read from global memory through L1 with explicit FP32 bilinear interpolation (the reference
+// used point-sampled layered textures); a sample is zero outside [0, W-1) x [0, H-1).
+// vol_out = vol_in + sum_p bilinear(proj_p; u, v) / w^2, x fastest.
+#include "common.h"
+
+namespace fdk {
+
+__global__ void __launch_bounds__(256) rtk_bp_kernel(const float *__restrict__ vol_in, float *__restrict__ vol_out,
+                                                     const float *__restrict__ proj, const float *__restrict__ mats,
+                                                     int W, int H, int n, int nx, int ny, int nz) {
+    __shared__ float sm[32 * 12];
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (int q = tid; q < n * 12; q += 256) sm[q] = mats[q];
+    __syncthreads();
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny) return;
+    const float fi = (float)i, fj = (float)j, fk = (float)k;
+    const long long frame = (long long)W * H;
+    float acc = 0.f;
+    for (int p = 0; p < n; p++) {
+        const float *m = sm + 12 * p;
+        const float x = fmaf(m[0], fi, fmaf(m[1], fj, fmaf(m[2], fk, m[3])));
+        const float y = fmaf(m[4], fi, fmaf(m[5], fj, fmaf(m[6], fk, m[7])));
+        const float rw = 1.0f / fmaf(m[8], fi, fmaf(m[9], fj, fmaf(m[10], fk, m[11])));
+        const float u = x * rw, v = y * rw;
+        float s = 0.f;
+        if (u >= 0.f && u < (float)(W - 1) && v >= 0.f && v < (float)(H - 1)) {
+            const float iu = floorf(u), iv = floorf(v);
+            const float du = u - iu, dv = v - iv;
+            const float *p0 = proj + p * frame + (long long)iv * W + (int)iu;
+            const float *p1 = p0 + W;
+            const float a = fmaf(du, __ldg(p0 + 1) - __ldg(p0), __ldg(p0));
+            const float b = fmaf(du, __ldg(p1 + 1) - __ldg(p1), __ldg(p1));
+            s = fmaf(dv, b - a, a);
+        }
+        acc = fmaf(s * rw, rw, acc);
+    }
+    const long long idx = i + ((long long)j + (long long)k * ny) * nx;
+    vol_out[idx] = vol_in[idx] + acc;
+}
+
+}  // namespace fdk
+
+using namespace fdk;
+
+extern "C" int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_size[3],
+                                            const float *matrices, const float *dev_vol_in, float *dev_vol_out,
+                                            const float *proj) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(proj_size && vol_size && matrices && dev_vol_in && dev_vol_out && proj, "NULL argument");
+    const int W = proj_size[0], H = proj_size[1], n = proj_size[2];
+    const int nx = vol_size[0], ny = vol_size[1], nz = vol_size[2];
+    FDK_CHECK_ARG(W > 1 && H > 1 && n > 0 && n <= 32, "proj_size out of range (views <= 32)");
+    FDK_CHECK_ARG(nx > 0 && ny > 0 && nz > 0 && nz <= 65535, "vol_size out of range");
+    const size_t bytes = sizeof(float) * (size_t)W * H * n;
+    float *d_proj = nullptr, *d_mats = nullptr;
+    FDK_CUDA(cudaMalloc(&d_proj, bytes));
+    int s = FDK_OK;
+    cudaError_t e = cudaMalloc(&d_mats, sizeof(float) * 12 * n);
+    if (e == cudaSuccess) e = cudaMemcpy(d_proj, proj, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_mats, matrices, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        const dim3 grid((unsigned)ceil_div(nx, 32), (unsigned)ceil_div(ny, 8), nz);
+        rtk_bp_kernel<<<grid, dim3(32, 8)>>>(dev_vol_in, dev_vol_out, d_proj, d_mats, W, H, n, nx, ny, nz);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) s = cuda_status(e, "CUDA_reconstruct_conebeam", __FILE__, __LINE__);
+    cudaFree(d_proj);
+    if (d_mats) cudaFree(d_mats);
+    return s;
+    FDK_ABI_END
+}

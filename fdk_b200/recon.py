@@ -1,0 +1,67 @@
+"""Reconstructor: end-to-end streaming FDK on one GPU (cosine weight, ramp filter,
+backprojection of the whole volume), the single-GPU form of cuFDK's filter -> BP handoff
+(cuFDK/mpiFDK.cpp:58-317)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import PRECISIONS, check, lib
+
+
+class Reconstructor:
+    def __init__(self, param, precision: str = "mixed", batch: int = 32, device: int = 0):
+        self.param = param
+        self.precision = precision
+        self._g = param.to_c()
+        self._h = C.c_void_p()
+        check(lib().fdk_recon_create(C.byref(self._h), C.byref(self._g), PRECISIONS[precision], batch, device))
+
+    def push(self, views: np.ndarray, first: int) -> None:
+        """Raw views (n, nv, nu) float32 in host memory (pinned memory overlaps best)."""
+        v = views
+        if v.dtype != np.float32 or not v.flags.c_contiguous:
+            raise ValueError("views must be C-contiguous float32")
+        n = v.shape[0]
+        check(lib().fdk_recon_push(self._h, v.ctypes.data, first, n))
+
+    def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
+        check(lib().fdk_recon_push(self._h, host_ptr, first, n))
+
+    def push_device(self, dev_ptr: int, first: int, n: int) -> None:
+        check(lib().fdk_recon_push_device(self._h, dev_ptr, first, n))
+
+    def sync(self, timeout_ms: int = 0) -> None:
+        check(lib().fdk_recon_sync(self._h, timeout_ms))
+
+    def volume(self, out: np.ndarray | None = None) -> np.ndarray:
+        p = self.param
+        n = p.nx * p.ny * p.nz
+        if out is None:
+            out = np.empty(n, np.float32)
+        check(lib().fdk_recon_get_volume(self._h, out.ctypes.data, n))
+        return out.reshape(p.nz, p.ny, p.nx)
+
+    def volume_into(self, host_ptr: int) -> None:
+        p = self.param
+        check(lib().fdk_recon_get_volume(self._h, host_ptr, p.nx * p.ny * p.nz))
+
+    def stats(self):
+        bp, fl, n = C.c_double(), C.c_double(), C.c_int64()
+        check(lib().fdk_recon_stats(self._h, C.byref(bp), C.byref(fl), C.byref(n)))
+        return {"bp_ms": bp.value, "filter_ms": fl.value, "views": n.value}
+
+    def reset(self) -> None:
+        check(lib().fdk_recon_reset(self._h))
+
+    def close(self):
+        if self._h:
+            lib().fdk_recon_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

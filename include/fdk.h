@@ -1,0 +1,235 @@
+/*
+ * fdk.h -- C ABI of the B200-native FDK reconstructor (libfdk_b200.so).
+ *
+ * The entry points replace the reference's plugin boundaries (peng-ac/fdk):
+ *   - the FDK geometry core   (common/type.h  Parameter, filter(), CalculateCosTable,
+ *                              CalculateProjMat)
+ *   - the CPU filter plugin   (Filterlib/FilterLib.h  FilterEngine)
+ *   - the GPU filter plugin   (FilterlibCufft/cudaFftFilter.cuh  FilterRow_Real32,
+ *                              CorrectImage_Real32)
+ *   - the backprojection      (cudaBP/backprojection.cuh  BackProjectionFDK)
+ *   - the RTK-style drop-in   (cudaBP/rtkCudaFDKBackProjectionImageFilter.cu
+ *                              CUDA_reconstruct_conebeam)
+ * Each declaration cites the reference interface it replaces.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only; no C++ or torch types cross this ABI.
+ *   - Every function returns an int status: FDK_OK (0) or a negative FDK_ERR_*.
+ *     Nothing throws across the ABI.  fdk_last_error() returns a thread-local
+ *     message for the last failing call on the calling thread.
+ *   - "host" pointers are CPU memory (pageable or pinned); "dev" pointers are
+ *     device memory on the handle's device.
+ *   - Handles are not thread-safe: one host thread drives one handle, as the
+ *     reference drives one BackProjectionFDK per GPU from one BpThread
+ *     (cuFDK/mpiFDK.cpp:205-317).
+ *   - stream arguments are cudaStream_t passed as void* (NULL = legacy default
+ *     stream).
+ */
+#ifndef FDK_B200_FDK_H
+#define FDK_B200_FDK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDK_ABI_VERSION 1
+
+/* ---- status codes --------------------------------------------------------- */
+#define FDK_OK 0
+#define FDK_ERR_INVALID_ARG (-1)   /* bad size, pointer, layout or state */
+#define FDK_ERR_CUDA (-2)          /* a CUDA runtime call failed */
+#define FDK_ERR_OUT_OF_MEMORY (-3) /* device or pinned-host allocation failed */
+#define FDK_ERR_TIMEOUT (-4)       /* a bounded wait (host or device) ran out */
+#define FDK_ERR_UNSUPPORTED (-5)   /* valid request this build does not implement */
+#define FDK_ERR_NO_DEVICE (-6)     /* no CUDA device visible */
+#define FDK_ERR_DEVICE_CHECK (-7)  /* a kernel reported an internal check failure */
+
+const char *fdk_last_error(void);
+int fdk_abi_version(void);
+/* Number of visible CUDA devices (0 without a GPU; not an error). */
+int fdk_device_count(int *count);
+
+/* ---- geometry: Parameter (common/type.h:4627-4895) ------------------------ */
+/* Filter windows, in the order of s_FILTER_TYPE (common/type.h:4619-4626). */
+#define FDK_FILTER_NONE 0
+#define FDK_FILTER_RAM_LAK 1
+#define FDK_FILTER_SHEPP_LOGAN 2
+#define FDK_FILTER_COSINE 3
+#define FDK_FILTER_HAMMING 4
+#define FDK_FILTER_HANN 5
+
+typedef struct fdk_geometry {
+    int64_t nx, ny, nz;          /* volume size in voxels */
+    double dx, dy, dz;           /* voxel pitch, mm */
+    int64_t nu, nv;              /* detector columns, rows */
+    double du, dv;               /* detector pitch, mm */
+    double offset_nu, offset_nv; /* detector offsets in pixels (cos table only, as in the reference) */
+    double sid;                  /* source-to-detector distance, mm (reference "SID") */
+    double sod;                  /* source-to-axis distance, mm (reference "SOD") */
+    int64_t direction;           /* rotation direction, +1 or -1 */
+    double scan_angle;           /* degrees covered by n_proj views */
+    int64_t n_proj;              /* number of views */
+    double volume_position_angle; /* radians added to every view angle (reference volume_postion_angle) */
+    int32_t filter_type;         /* FDK_FILTER_* */
+    int32_t reserved;
+} fdk_geometry;
+
+/* Parameter::Parameter() defaults (common/type.h:4628-4662). */
+void fdk_geometry_default(fdk_geometry *g);
+/* nextpow2 (common/type.h:4418-4425): filter length W for nu columns (doubles exact powers of two). */
+int64_t fdk_filter_length(int64_t nu);
+/* filter(strType, len, d) (common/type.h:4427-4475): W = fdk_filter_length(len) FP64 taps of the
+ * frequency response, written to out (capacity out_len >= W). */
+int fdk_filter_design(int32_t filter_type, int64_t len, int32_t d, double *out, int64_t out_len);
+/* AngularAndrampFactor (common/type.h:4736). */
+int fdk_angular_ramp_factor(const fdk_geometry *g, double *out);
+/* cos_sigma table, nv rows of nu (CalculateCosTable, common/type.h:4756-4783):
+ * SID/sqrt(u^2+v^2+SID^2) * SOD^2 * AngularAndrampFactor, FP32 storage. */
+int fdk_cos_table(const fdk_geometry *g, float *out);
+/* Per-view angles in radians: direction*deg/180*pi + volume_position_angle, deg = i*scan_angle/n_proj
+ * (common/type.h:4729, 4824). */
+int fdk_view_angles(const fdk_geometry *g, double *out);
+/* 3x4 projection matrices, 12 per view, row major (CalculateProjMat, common/type.h:4898-4944;
+ * vec_rot_mat_ijk3x4 4821-4831).  Computed in FP64; out_f64 and/or out_f32 may be NULL. */
+int fdk_projection_matrices(const fdk_geometry *g, double *out_f64, float *out_f32);
+
+/* ---- filter: FilterEngine (Filterlib/FilterLib.h:148-203) ----------------- */
+/* Output element type of the device filter. */
+#define FDK_DTYPE_F32 0
+#define FDK_DTYPE_F16 1
+/* Output layout of the device filter.
+ *   ROWS       nv rows of nu (the input layout; FilterEngine transpose=false)
+ *   TRANSPOSED nu rows of nv  (FilterEngine transpose=true; the BackProjectionFDK input)
+ *   MIRROR     nu rows of nv mirror pairs: element (u, v) holds the filtered values of detector
+ *              rows v and nv-1-v.  This is the backprojection's internal staging layout. */
+#define FDK_LAYOUT_ROWS 0
+#define FDK_LAYOUT_TRANSPOSED 1
+#define FDK_LAYOUT_MIRROR 2
+
+typedef struct fdk_filter fdk_filter;
+/* FilterEngine(cos_image_table, fft_kernel_real_f32) (FilterLib.h:152-164).
+ * cos_table: host, nv rows of nu (NULL = no cosine weighting).  H: host, W taps.
+ * pad_edge: samples averaged for the constant edge pad -- 4 as the IPP plugin
+ * (FilterLib.h:38,44), 3 as the cuFFT plugin (cudaFftFilter.cu:25,29).
+ * W must be a power of two, nu <= W <= 4096. */
+int fdk_filter_create(fdk_filter **out, const float *cos_table, const float *H, int64_t nu, int64_t nv,
+                      int64_t W, int32_t pad_edge, int32_t device);
+/* FilterEngine::Filtering(src, dst, transpose) (FilterLib.h:167-196): one view, host buffers.
+ * As in the reference, src is cosine-weighted in place.  dst is nv x nu, or nu x nv if transpose. */
+int fdk_filter_filtering(fdk_filter *h, float *src_host, float *dst_host, int32_t transpose);
+/* Device batch: n_views views (nv x nu each, contiguous) -> dst in `layout` and `out_dtype`.
+ * Cosine weighting is applied on the fly (src is not modified).  Asynchronous on stream. */
+int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, int64_t n_views,
+                          int32_t layout, int32_t out_dtype, void *stream);
+int fdk_filter_destroy(fdk_filter *h);
+
+/* FilterlibCufft plugin (FilterlibCufft/cudaFftFilter.cuh:6-8, cudaFftFilter.cu:283-392).
+ * DataRef<float> (FilterlibCufft/cudaBackProjection.cuh:121-230) as a plain struct: device data,
+ * width (fast axis), height, depth, pitch in elements.
+ * fdk_correct_image_real32: dst = src * table per view (kernelCorrect, cudaFftFilter.cu:270-281).
+ * fdk_filter_row_real32: ramp filter of every row of every view with the W-tap response in
+ * `filter` (pad with the mean of 3 edge samples, cudaFftFilter.cu:14-61).  Synchronous, as the
+ * reference. */
+typedef struct fdk_dataref {
+    float *data;
+    int32_t width, height, depth, pitch;
+} fdk_dataref;
+int fdk_correct_image_real32(const fdk_dataref *src, const fdk_dataref *table, fdk_dataref *dst);
+int fdk_filter_row_real32(const fdk_dataref *src, fdk_dataref *dst, const fdk_dataref *filter);
+
+/* ---- backprojection: BackProjectionFDK (cudaBP/backprojection.cuh:246-271) -- */
+/* Arithmetic of the backprojection kernel.
+ *   FP32_EXACT  the reference kernel's arithmetic (cudaFdkBP, backprojectionFDK.cu:50-129:
+ *               FP32, mad.rz.ftz blends), bit-identical results; views read through L1.
+ *   FP32        FP32 views staged in shared memory, FP32 accumulation (plain FP32 fast path).
+ *   MIXED       FP16 views staged in shared memory, FP32 compensated accumulation. */
+#define FDK_BP_FP32_EXACT 0
+#define FDK_BP_FP32 1
+#define FDK_BP_MIXED 2
+
+/* geo::BoxT<size_t> (cudaBP/backprojection.cuh:66-116): origin and extent in voxels. */
+typedef struct fdk_box {
+    uint64_t x, y, z, width, height, depth;
+} fdk_box;
+
+typedef struct fdk_bp fdk_bp;
+/* BackProjectionFDK(projW, projH, projCount, nx, ny, nz, subTop, subBottom)
+ * (backprojectionFDK.cu:161-227).  proj_width/proj_height: the transposed view (width = nv,
+ * height = nu, cuFDK/mpiFDK.cpp:196).  proj_count: views per BP() call (<= 32 as MAX_PROJ).
+ * sub_bottom->depth > 0 selects the mirror-symmetric slab pair; then
+ * sub_top->z + sub_bottom->z + sub_bottom->depth - 1 == nz - 1 (:171-173).
+ * The volume is zeroed on creation. */
+int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t proj_count,
+                  int32_t nx, int32_t ny, int32_t nz, const fdk_box *sub_top,
+                  const fdk_box *sub_bottom, int32_t precision, int32_t device);
+/* BP(TRANSPOSE, pProjData, width, height, pProjMat, nProj) (backprojectionFDK.cu:229-276).
+ * host_proj: n_proj views, host memory; copied before return, so the caller may reuse it.
+ * transpose = 1: views are height (= nu) rows of width (= nv) values, the production layout.
+ * transpose = 0: views are nv rows of nu.  proj_mat: 12 floats per view (host). */
+int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t width, int32_t height,
+              const float *proj_mat, int32_t n_proj);
+/* Device-resident variant: views already on the device in FDK_LAYOUT_TRANSPOSED (f32) or
+ * FDK_LAYOUT_MIRROR (f32 or f16 per the handle's precision), n_proj <= 128.  Asynchronous on
+ * stream; dev_proj must stay valid until the stream passes this call. */
+int fdk_bp_bp_device(fdk_bp *h, const void *dev_proj, int32_t layout, const float *proj_mat,
+                     int32_t n_proj, void *stream);
+/* GetVolumeData(pVol, size) (backprojectionFDK.cu:278-362): writes the sub-volume as
+ * [zs][y][x] (x fastest), zs = top slab then bottom slab, each ascending.  Synchronous. */
+int fdk_bp_get_volume(fdk_bp *h, float *host_vol, int64_t size);
+/* Device pointer of the internal volume ([x][y][zs], zs fastest) and its size in floats. */
+int fdk_bp_volume_device(fdk_bp *h, float **dev_vol, int64_t *count);
+/* nBpCount, fKernelTime (cudaBP/backprojection.cuh:130, 265): views backprojected and the summed
+ * kernel time in ms (events on the handle's stream). */
+int fdk_bp_stats(fdk_bp *h, int64_t *bp_count, double *kernel_ms);
+/* Zero the volume (start a new reconstruction with the same handle). */
+int fdk_bp_reset(fdk_bp *h);
+int fdk_bp_destroy(fdk_bp *h);
+
+/* ---- RTK drop-in: CUDA_reconstruct_conebeam
+ *      (cudaBP/rtkCudaFDKBackProjectionImageFilter.cu:200-330) ---------------- */
+/* proj_size = {width (u), height (v), n_proj <= 32}, vol_size = {nx, ny, nz}.
+ * matrices: host, 12 floats per view (index -> (u*w, v*w, w)).  dev_vol_in/dev_vol_out: device,
+ * x fastest; dev_vol_out = dev_vol_in + sum_p bilinear(proj_p; u, v) / w^2.  proj: HOST views,
+ * u fastest (the reference copies it with cudaMemcpyHostToDevice, :256).  Synchronous. */
+int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_size[3],
+                                 const float *matrices, const float *dev_vol_in, float *dev_vol_out,
+                                 const float *proj);
+
+/* ---- end-to-end streaming FDK (single-GPU analogue of cuFDK's
+ *      FilterThread -> BpThread handoff, cuFDK/mpiFDK.cpp:58-317) ------------- */
+typedef struct fdk_recon fdk_recon;
+/* A reconstructor for geometry g: cosine weight + ramp filter + backprojection of the whole
+ * volume (mirror slab pair, as DivVolume with one rank, cuFDK/mpiFDK.h:116-149).
+ * batch: views per internal batch (multiple of 2, <= 128).  precision: FDK_BP_*. */
+int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch,
+                     int32_t device);
+/* Push n raw views (host, nv x nu each, index first..first+n-1; pinned memory overlaps best).
+ * The copy to the device runs on a side stream; filtering and backprojection follow on the
+ * compute stream.  Returns once the host buffer may be reused. */
+int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t n);
+/* Push n raw views already in device memory (nv x nu each). */
+int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n);
+/* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
+int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
+/* Volume [z][y][x], x fastest, nz*ny*nx floats (host).  Implies fdk_recon_sync. */
+int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size);
+/* Timing: total BP kernel ms, total filter kernel ms, views done. */
+int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views);
+int fdk_recon_reset(fdk_recon *h);
+int fdk_recon_destroy(fdk_recon *h);
+
+/* ---- synthetic data: analytic ellipsoid projections on the device ---------- */
+/* ell: host, n_ell records of 16 doubles {cx, cy, cz, a, b, c, R00..R22, rho} in the world frame
+ * of CalculateProjMat (X = (x-(nx-1)/2)dx, Y = -(y-(ny-1)/2)dy, Z = -(z-(nz-1)/2)dz, mm;
+ * world = R * local).  Writes n views (first..first+n-1) of exact line integrals, nv x nu each,
+ * to dev_out (f32).  Asynchronous on stream. */
+int fdk_phantom_project(const fdk_geometry *g, const double *ell, int32_t n_ell, int64_t first,
+                        int64_t n, float *dev_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDK_B200_FDK_H */
