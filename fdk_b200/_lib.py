@@ -40,9 +40,9 @@ EXPORTED = [
     "fdk_bp_create", "fdk_bp_bp", "fdk_bp_bp_device", "fdk_bp_get_volume", "fdk_bp_volume_device",
     "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
     "fdk_rtk_reconstruct_conebeam",
-    "fdk_recon_create", "fdk_recon_push", "fdk_recon_push_device", "fdk_recon_sync",
+    "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device", "fdk_recon_sync",
     "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_reset", "fdk_recon_destroy",
-    "fdk_phantom_project",
+    "fdk_phantom_project", "fdk_probe_smem", "fdk_probe_fma",
 ]
 
 
@@ -121,6 +121,8 @@ def lib() -> C.CDLL:
         "fdk_bp_destroy": ([vp], C.c_int),
         "fdk_rtk_reconstruct_conebeam": ([vp, vp, vp, vp, vp, vp], C.c_int),
         "fdk_recon_create": ([C.POINTER(vp), G, i32, i32, i32], C.c_int),
+        "fdk_recon_create_slab": ([C.POINTER(vp), G, i64, i64, i32, i32, i32], C.c_int),
+        "fdk_recon_stream": ([vp, C.POINTER(vp)], C.c_int),
         "fdk_recon_push": ([vp, vp, i64, i64], C.c_int),
         "fdk_recon_push_device": ([vp, vp, i64, i64], C.c_int),
         "fdk_recon_sync": ([vp, i64], C.c_int),
@@ -129,6 +131,8 @@ def lib() -> C.CDLL:
         "fdk_recon_reset": ([vp], C.c_int),
         "fdk_recon_destroy": ([vp], C.c_int),
         "fdk_phantom_project": ([G, vp, i32, i64, i64, vp, vp], C.c_int),
+        "fdk_probe_smem": ([i32, f64p], C.c_int),
+        "fdk_probe_fma": ([i32, f64p], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -142,6 +146,14 @@ def check(rc: int) -> None:
     if rc != FDK_OK:
         msg = lib().fdk_last_error()
         raise FdkError(rc, msg.decode() if msg else "")
+
+
+def probe_peaks(device: int = 0) -> dict:
+    """Measured shared-memory bandwidth (GB/s) and FP32 FMA rate (TFLOP/s) of the device."""
+    a, b = C.c_double(), C.c_double()
+    check(lib().fdk_probe_smem(device, C.byref(a)))
+    check(lib().fdk_probe_fma(device, C.byref(b)))
+    return {"smem_gbs": a.value, "fp32_tflops": b.value}
 
 
 def device_count() -> int:

@@ -155,7 +155,7 @@ struct fdk_bp {
     const float *ext_scale = nullptr;  // accumulator scale of FP16 views pushed by the reconstructor
 };
 
-namespace {
+namespace bpi {
 
 int collect_timers(fdk_bp *h) {
     for (auto &t : h->timers) {
@@ -234,7 +234,9 @@ int check_circular(const float *mats, int n) {
     return FDK_OK;
 }
 
-}  // namespace
+}  // namespace bpi
+
+using namespace bpi;
 
 extern "C" {
 
@@ -490,4 +492,20 @@ int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale) {
     if (!h) return FDK_ERR_INVALID_ARG;
     h->ext_scale = d_scale;
     return FDK_OK;
+}
+
+// Backprojection of device-resident views with device-resident matrices, for the
+// reconstructor (recon.cu): no host round trip per batch, so consecutive batches queue on the
+// stream without the host waiting for the GPU.  Internal to the library.
+int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
+                                   int32_t n_proj, const float *host_mats, void *stream) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h && dev_proj && dev_mats && host_mats, "NULL argument");
+    FDK_CHECK_ARG(n_proj > 0 && n_proj <= 128, "n_proj %d outside 1..128", n_proj);
+    if (h->precision != FDK_BP_FP32_EXACT) FDK_TRY(check_circular(host_mats, n_proj));
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    return launch_bp(h, dev_proj, layout, 1, dev_mats, n_proj, h->proj_w, h->proj_h, (cudaStream_t)stream,
+                     h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr);
+    FDK_ABI_END
 }

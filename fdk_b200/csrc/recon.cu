@@ -36,6 +36,7 @@ struct fdk_recon {
     unsigned int *d_overflow = nullptr;
     float out_scale = 1.0f;
     std::vector<float> mats;         // 12 x n_proj, FP32 (from FP64)
+    float *d_mats = nullptr;         // the same on the device
     cudaStream_t compute = nullptr, copy = nullptr;
     cudaEvent_t raw_ready[2] = {nullptr, nullptr}, raw_free[2] = {nullptr, nullptr};
     cudaEvent_t f0 = nullptr, f1 = nullptr, done = nullptr;
@@ -45,8 +46,10 @@ struct fdk_recon {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
 };
 
-// fast-path accumulator scale hook (bp.cu)
+// internal hooks (bp.cu)
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
+int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
+                                   int32_t n_proj, const float *host_mats, void *stream);
 
 namespace {
 
@@ -67,6 +70,7 @@ int recon_release(fdk_recon *h) {
         cudaEventDestroy(t.second);
     }
     if (h->d_cos) cudaFree(h->d_cos);
+    if (h->d_mats) cudaFree(h->d_mats);
     if (h->d_filt) cudaFree(h->d_filt);
     if (h->d_scale) cudaFree(h->d_scale);
     if (h->d_overflow) cudaFree(h->d_overflow);
@@ -106,7 +110,8 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
     h->ftimers.push_back(t);
     if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
     if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
-    FDK_TRY(fdk_bp_bp_device(h->bp, h->d_filt, h->layout, h->mats.data() + 12 * first, n, h->compute));
+    FDK_TRY(fdk_bp_bp_device_mats_internal(h->bp, h->d_filt, h->layout, h->d_mats + 12 * first, n,
+                                           h->mats.data() + 12 * first, h->compute));
     h->views += n;
     return FDK_OK;
 }
@@ -116,6 +121,18 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
 extern "C" {
 
 int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch, int32_t device) {
+    FDK_CHECK_ARG(g != nullptr, "NULL geometry");
+    return fdk_recon_create_slab(out, g, 0, g->nz / 2, precision, batch, device);
+}
+
+int fdk_recon_stream(fdk_recon *h, void **stream) {
+    FDK_CHECK_ARG(h && stream, "NULL argument");
+    *stream = (void *)h->compute;
+    return FDK_OK;
+}
+
+int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z, int64_t depth, int32_t precision,
+                          int32_t batch, int32_t device) {
     FDK_ABI_BEGIN
     clear_error();
     FDK_CHECK_ARG(out && g, "NULL argument");
@@ -123,6 +140,8 @@ int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, 
     FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
     FDK_CHECK_ARG(batch > 0 && batch <= 128, "batch must be 1..128");
     FDK_CHECK_ARG(g->nz % 2 == 0, "the slab-pair reconstructor needs an even nz");
+    FDK_CHECK_ARG(depth > 0 && top_z >= 0 && top_z + depth <= g->nz / 2, "slab [%lld, %lld) outside the top half",
+                  (long long)top_z, (long long)(top_z + depth));
     FDK_CHECK_ARG(g->nx <= 65535 * 16 && g->ny <= 65535 * 16, "volume too large");
     const int64_t W = fdk_filter_length(g->nu);
     FDK_CHECK_ARG(W <= 4096, "detector too wide: nextpow2(nu) = %lld > 4096", (long long)W);
@@ -151,6 +170,9 @@ int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, 
     const long long frame = g->nu * g->nv;
     if (s == FDK_OK) ck(cudaMalloc(&h->d_cos, sizeof(float) * frame), "cos table");
     if (s == FDK_OK) ck(cudaMemcpy(h->d_cos, cos.data(), sizeof(float) * frame, cudaMemcpyHostToDevice), "cos copy");
+    if (s == FDK_OK) ck(cudaMalloc(&h->d_mats, sizeof(float) * h->mats.size()), "matrices");
+    if (s == FDK_OK)
+        ck(cudaMemcpy(h->d_mats, h->mats.data(), sizeof(float) * h->mats.size(), cudaMemcpyHostToDevice), "matrices");
     for (int i = 0; i < 2 && s == FDK_OK; i++) {
         ck(cudaMalloc(&h->d_raw[i], sizeof(float) * frame * batch), "raw views");
         ck(cudaEventCreateWithFlags(&h->raw_ready[i], cudaEventDisableTiming), "event");
@@ -174,9 +196,9 @@ int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, 
         if (s == FDK_OK) ck(cudaMemcpy(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice), "scale");
     }
     if (s == FDK_OK) {
-        const uint64_t half = g->nz / 2;
-        fdk_box top{0, 0, 0, (uint64_t)g->nx, (uint64_t)g->ny, half};
-        fdk_box bot{0, 0, half, (uint64_t)g->nx, (uint64_t)g->ny, half};
+        const uint64_t d = (uint64_t)depth, z0 = (uint64_t)top_z;
+        fdk_box top{0, 0, z0, (uint64_t)g->nx, (uint64_t)g->ny, d};
+        fdk_box bot{0, 0, (uint64_t)g->nz - z0 - d, (uint64_t)g->nx, (uint64_t)g->ny, d};
         s = fdk_bp_create(&h->bp, (int)g->nv, (int)g->nu, precision == FDK_BP_FP32_EXACT ? 32 : batch, (int)g->nx,
                           (int)g->ny, (int)g->nz, &top, &bot, precision, device);
         if (s == FDK_OK && h->d_scale) s = fdk_bp_set_acc_scale_internal(h->bp, h->d_scale);

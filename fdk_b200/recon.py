@@ -1,6 +1,8 @@
 """Reconstructor: end-to-end streaming FDK on one GPU (cosine weight, ramp filter,
-backprojection of the whole volume), the single-GPU form of cuFDK's filter -> BP handoff
-(cuFDK/mpiFDK.cpp:58-317)."""
+backprojection), the single-GPU form of cuFDK's filter -> BP handoff (cuFDK/mpiFDK.cpp:58-317).
+
+The whole volume is reconstructed as one mirror-symmetric slab pair; with ``slab=(top_z,
+depth)`` only that pair (one rank of DivVolume, see ``fdk_b200.shard``)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -11,20 +13,33 @@ from ._lib import PRECISIONS, check, lib
 
 
 class Reconstructor:
-    def __init__(self, param, precision: str = "mixed", batch: int = 32, device: int = 0):
+    def __init__(self, param, precision: str = "mixed", batch: int = 32, device: int = 0, slab=None):
         self.param = param
         self.precision = precision
         self._g = param.to_c()
         self._h = C.c_void_p()
-        check(lib().fdk_recon_create(C.byref(self._h), C.byref(self._g), PRECISIONS[precision], batch, device))
+        if slab is None:
+            slab = (0, param.nz // 2)
+        self.slab = (int(slab[0]), int(slab[1]))
+        check(lib().fdk_recon_create_slab(C.byref(self._h), C.byref(self._g), self.slab[0], self.slab[1],
+                                          PRECISIONS[precision], batch, device))
+
+    @property
+    def depth(self) -> int:
+        """Storage depth of the slab pair (top + bottom)."""
+        return 2 * self.slab[1]
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().fdk_recon_stream(self._h, C.byref(s)))
+        return s.value or 0
 
     def push(self, views: np.ndarray, first: int) -> None:
         """Raw views (n, nv, nu) float32 in host memory (pinned memory overlaps best)."""
-        v = views
-        if v.dtype != np.float32 or not v.flags.c_contiguous:
+        if views.dtype != np.float32 or not views.flags.c_contiguous:
             raise ValueError("views must be C-contiguous float32")
-        n = v.shape[0]
-        check(lib().fdk_recon_push(self._h, v.ctypes.data, first, n))
+        check(lib().fdk_recon_push(self._h, views.ctypes.data, first, views.shape[0]))
 
     def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push(self._h, host_ptr, first, n))
@@ -36,16 +51,17 @@ class Reconstructor:
         check(lib().fdk_recon_sync(self._h, timeout_ms))
 
     def volume(self, out: np.ndarray | None = None) -> np.ndarray:
+        """[zs][y][x]: the full volume [z][y][x] for the default slab pair."""
         p = self.param
-        n = p.nx * p.ny * p.nz
+        n = p.nx * p.ny * self.depth
         if out is None:
             out = np.empty(n, np.float32)
         check(lib().fdk_recon_get_volume(self._h, out.ctypes.data, n))
-        return out.reshape(p.nz, p.ny, p.nx)
+        return out.reshape(self.depth, p.ny, p.nx)
 
     def volume_into(self, host_ptr: int) -> None:
         p = self.param
-        check(lib().fdk_recon_get_volume(self._h, host_ptr, p.nx * p.ny * p.nz))
+        check(lib().fdk_recon_get_volume(self._h, host_ptr, p.nx * p.ny * self.depth))
 
     def stats(self):
         bp, fl, n = C.c_double(), C.c_double(), C.c_int64()

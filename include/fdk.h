@@ -206,6 +206,14 @@ typedef struct fdk_recon fdk_recon;
  * batch: views per internal batch (multiple of 2, <= 128).  precision: FDK_BP_*. */
 int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch,
                      int32_t device);
+/* The same for one mirror-symmetric slab pair of the volume (one rank of DivVolume,
+ * cuFDK/mpiFDK.h:116-149): top slab z in [top_z, top_z + depth), bottom slab
+ * z in [nz - top_z - depth, nz - top_z).  fdk_recon_get_volume then returns the pair as
+ * [zs][y][x] with zs = top slab then bottom slab, ascending. */
+int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z, int64_t depth,
+                          int32_t precision, int32_t batch, int32_t device);
+/* The reconstructor's compute stream (cudaStream_t as void*), for event timing by the caller. */
+int fdk_recon_stream(fdk_recon *h, void **stream);
 /* Push n raw views (host, nv x nu each, index first..first+n-1; pinned memory overlaps best).
  * The copy to the device runs on a side stream; filtering and backprojection follow on the
  * compute stream.  Returns once the host buffer may be reused. */
@@ -214,7 +222,8 @@ int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t
 int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
-/* Volume [z][y][x], x fastest, nz*ny*nx floats (host).  Implies fdk_recon_sync. */
+/* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).
+ * Implies fdk_recon_sync. */
 int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size);
 /* Timing: total BP kernel ms, total filter kernel ms, views done. */
 int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views);
@@ -228,6 +237,13 @@ int fdk_recon_destroy(fdk_recon *h);
  * to dev_out (f32).  Asynchronous on stream. */
 int fdk_phantom_project(const fdk_geometry *g, const double *ell, int32_t n_ell, int64_t first,
                         int64_t n, float *dev_out, void *stream);
+
+/* ---- measurement probes (no reference counterpart) ------------------------ */
+/* The backprojection is bound by shared-memory bandwidth or FP32 issue rate; these measure the
+ * two denominators of its roofline on the given device: conflict-free 128-bit shared-memory
+ * loads on every SM (GB/s) and independent FP32 FMA chains on every SM (TFLOP/s). */
+int fdk_probe_smem(int32_t device, double *gbs);
+int fdk_probe_fma(int32_t device, double *tflops);
 
 #ifdef __cplusplus
 }

@@ -195,7 +195,28 @@ class RefCPU:
                                    [C.c_double] * 4 + [C.c_long, C.c_double, C.c_long, C.c_double,
                                                        C.c_int, _f32p, C.c_int, C.c_int, _f32p,
                                                        C.c_int])
+        L.refc_fdk_create.restype = C.c_void_p
+        L.refc_fdk_create.argtypes = ([C.c_long] * 3 + [C.c_double] * 3 + [C.c_long] * 2 +
+                                      [C.c_double] * 4 + [C.c_long, C.c_double, C.c_long, C.c_double,
+                                                          C.c_int])
+        L.refc_fdk_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.refc_fdk_destroy.argtypes = [C.c_void_p]
         self.L = L
+
+    def fdk_handle(self, g, ftype="hann"):
+        """Persistent reference CPU FDK (tables and buffers built once, outside timing)."""
+        h = self.L.refc_fdk_create(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.nu, g.nv, g.du, g.dv, g.SID,
+                                   g.SOD, g.direction, g.scan_angle, g.nProj, g.volume_postion_angle,
+                                   FILTERS[ftype])
+        assert h, "refc_fdk_create failed"
+        return h
+
+    def fdk_run(self, h, proj: np.ndarray, first: int, threads: int = 0) -> None:
+        proj = np.ascontiguousarray(proj, np.float32)
+        assert self.L.refc_fdk_run(h, proj.ctypes.data, int(first), int(proj.shape[0]), int(threads)) == 0
+
+    def fdk_destroy(self, h) -> None:
+        self.L.refc_fdk_destroy(h)
 
     def parameter(self, g, ftype="hann"):
         W = nextpow2(g.nu)

@@ -86,3 +86,53 @@ extern "C" int refc_cpu_fdk(long nx, long ny, long nz, double dx, double dy, dou
         return -1;
     }
 }
+
+// Persistent form for timing: the Parameter (init() builds every table) and the volume and
+// count buffers are set up once, outside the timed calls.
+struct RefFdk {
+    Parameter p;
+    Volume *vol = nullptr;
+    VolumeT<ushort> *cnt = nullptr;
+};
+
+extern "C" void* refc_fdk_create(long nx, long ny, long nz, double dx, double dy, double dz,
+                                 long nu, long nv, double du, double dv, double sid, double sod,
+                                 long direction, double scan_angle, long nproj, double vpa, int filter_type) {
+    try {
+        RefFdk* h = new RefFdk();
+        fill_param(h->p, nx, ny, nz, dx, dy, dz, nu, nv, du, dv, 0, 0, sid, sod, direction, scan_angle,
+                   nproj, vpa, filter_type);
+        h->vol = new Volume(nx, ny, nz);
+        h->cnt = new VolumeT<ushort>(nx, ny, nz);
+        return h;
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+// Backproject (with cos weighting and filtering, as BackProjection does) views
+// [first, first+count) from `proj`; threads <= 0: all.
+extern "C" int refc_fdk_run(void* hv, const float* proj, int first, int count, int threads) {
+    try {
+        RefFdk* h = static_cast<RefFdk*>(hv);
+        if (threads > 0) omp_set_num_threads(threads);
+        const long nu = h->p.nu, nv = h->p.nv;
+        for (int s = 0; s < count; s++) {
+            const int idx = first + s;
+            FrameT<float> fr(const_cast<float*>(proj) + (size_t)s * nu * nv, (int)nu, (int)nv, idx);
+            const double angle_rad = h->p.direction * h->p.vec_deg[idx] / 180.0 * PI + h->p.volume_postion_angle;
+            if (!BackProjection<float>(fr, h->p, angle_rad, *h->vol, *h->cnt)) return -3;
+        }
+        return 0;
+    } catch (...) {
+        return -1;
+    }
+}
+
+extern "C" void refc_fdk_destroy(void* hv) {
+    RefFdk* h = static_cast<RefFdk*>(hv);
+    if (!h) return;
+    delete h->vol;
+    delete h->cnt;
+    delete h;
+}
