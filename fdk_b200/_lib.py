@@ -106,7 +106,7 @@ def lib() -> C.CDLL:
         "fdk_projection_matrices": ([G, vp, vp], C.c_int),
         "fdk_filter_create": ([C.POINTER(vp), vp, vp, i64, i64, i64, i32, i32], C.c_int),
         "fdk_filter_filtering": ([vp, vp, vp, i32], C.c_int),
-        "fdk_filter_run_device": ([vp, vp, vp, i64, i32, i32, vp], C.c_int),
+        "fdk_filter_run_device": ([vp, vp, vp, i64, i32, i32, C.c_float, vp], C.c_int),
         "fdk_filter_destroy": ([vp], C.c_int),
         "fdk_correct_image_real32": ([C.POINTER(DataRef)] * 3, C.c_int),
         "fdk_filter_row_real32": ([C.POINTER(DataRef)] * 3, C.c_int),

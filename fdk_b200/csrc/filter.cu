@@ -343,7 +343,7 @@ int fdk_filter_filtering(fdk_filter *h, float *src_host, float *dst_host, int32_
 }
 
 int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, int64_t n_views, int32_t layout,
-                          int32_t out_dtype, void *stream) {
+                          int32_t out_dtype, float out_scale, void *stream) {
     FDK_ABI_BEGIN
     clear_error();
     FDK_CHECK_ARG(h && src_dev && dst_dev, "NULL argument");
@@ -357,7 +357,7 @@ int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, in
     const long long dstride = layout == FDK_LAYOUT_MIRROR ? 2 * n : n;
     return filter_views(src_dev, (int)h->nu, n, dst_dev, dpitch, dstride, h->d_cos, (int)h->nu, h->tables,
                         (int)h->nu, (int)h->nv, h->pad, (int)n_views, layout, out_dtype,
-                        (cudaStream_t)stream);
+                        (cudaStream_t)stream, out_scale, nullptr);
     FDK_ABI_END
 }
 

@@ -44,9 +44,10 @@ class FilterEngine:
         return self
 
     def run_device(self, src_ptr: int, dst_ptr: int, n_views: int, layout: int = LAYOUT_TRANSPOSED,
-                   dtype: int = DTYPE_F32, stream: int = 0) -> None:
-        """Batch filter on device buffers (cosine weight applied on the fly)."""
-        check(lib().fdk_filter_run_device(self._h, src_ptr, dst_ptr, n_views, layout, dtype, stream))
+                   dtype: int = DTYPE_F32, out_scale: float = 1.0, stream: int = 0) -> None:
+        """Batch filter on device buffers (cosine weight applied on the fly); every output
+        sample is multiplied by out_scale (keep FP16 outputs in range)."""
+        check(lib().fdk_filter_run_device(self._h, src_ptr, dst_ptr, n_views, layout, dtype, out_scale, stream))
 
     def close(self):
         if self._h:

@@ -120,10 +120,11 @@ int fdk_filter_create(fdk_filter **out, const float *cos_table, const float *H, 
 /* FilterEngine::Filtering(src, dst, transpose) (FilterLib.h:167-196): one view, host buffers.
  * As in the reference, src is cosine-weighted in place.  dst is nv x nu, or nu x nv if transpose. */
 int fdk_filter_filtering(fdk_filter *h, float *src_host, float *dst_host, int32_t transpose);
-/* Device batch: n_views views (nv x nu each, contiguous) -> dst in `layout` and `out_dtype`.
- * Cosine weighting is applied on the fly (src is not modified).  Asynchronous on stream. */
+/* Device batch: n_views views (nv x nu each, contiguous) -> dst in `layout` and `out_dtype`,
+ * every output sample multiplied by out_scale (FP16 range control; 1 = none).  Cosine
+ * weighting is applied on the fly (src is not modified).  Asynchronous on stream. */
 int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, int64_t n_views,
-                          int32_t layout, int32_t out_dtype, void *stream);
+                          int32_t layout, int32_t out_dtype, float out_scale, void *stream);
 int fdk_filter_destroy(fdk_filter *h);
 
 /* FilterlibCufft plugin (FilterlibCufft/cudaFftFilter.cuh:6-8, cudaFftFilter.cu:283-392).

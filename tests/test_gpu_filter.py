@@ -41,11 +41,12 @@ def test_device_layouts():
     m = torch.empty((6, 80, 64, 2), dtype=torch.float32, device="cuda")
     eng.run_device(src.data_ptr(), m.data_ptr(), 6, F.LAYOUT_MIRROR, F.DTYPE_F32)
     h = torch.empty((6, 80, 64, 2), dtype=torch.float16, device="cuda")
-    eng.run_device(src.data_ptr(), h.data_ptr(), 6, F.LAYOUT_MIRROR, F.DTYPE_F16)
+    scale = float(1.0 / p.cos_sigma.max())  # back to line-integral units, inside the FP16 range
+    eng.run_device(src.data_ptr(), h.data_ptr(), 6, F.LAYOUT_MIRROR, F.DTYPE_F16, scale)
     r = torch.empty((6, 64, 80), dtype=torch.float32, device="cuda")
     eng.run_device(src.data_ptr(), r.data_ptr(), 6, F.LAYOUT_ROWS, F.DTYPE_F32)
     torch.cuda.synchronize()
-    t, m, h, r = t.cpu().numpy(), m.cpu().numpy(), h.float().cpu().numpy(), r.cpu().numpy()
+    t, m, h, r = t.cpu().numpy(), m.cpu().numpy(), h.float().cpu().numpy() / scale, r.cpu().numpy()
     assert max_rel(t, want) <= 2e-6
     assert np.array_equal(r.transpose(0, 2, 1), t)
     assert np.array_equal(m[..., 0], t) and np.array_equal(m[..., 1], t[:, :, ::-1])

@@ -69,12 +69,16 @@ def test_reconstruction_recovers_density():
     vol = r.volume()
     from fdk_b200.phantom import voxelize
 
+    from scipy import ndimage
+
     truth = voxelize(p, ell)
-    core = truth > 0.5
-    inner = np.zeros_like(core)
-    inner[n // 4:-n // 4, n // 4:-n // 4, n // 4:-n // 4] = True
-    assert abs(vol[core & inner].mean() - 1.0) < 0.03, vol[core & inner].mean()
-    assert abs(vol[~core & inner].mean()) < 0.03
+    core = ndimage.binary_erosion(truth > 0.5, iterations=3)
+    outside = ndimage.binary_erosion(truth < 0.5, iterations=3)
+    # The reference's discrete ramp (H[k] = 2k/W with H[0] = 0, common/type.h:4436) and
+    # normalisation reconstruct a uniform interior at about 0.95 of its density in this
+    # geometry (the FP64 oracle pipeline gives 0.951); the GPU result must match that.
+    assert 0.93 < vol[core].mean() < 0.97, vol[core].mean()
+    assert vol[core].std() < 0.02 and abs(vol[outside].mean()) < 0.03
 
 
 def test_linearity_and_reset():
