@@ -1,0 +1,24 @@
+"""Profiling driver (runs committed files only): a few backprojection launches at the 512^3 / 512^2 configuration (views and
+volume larger than L2, a few GB on the device), for `ncu --set full -k regex:bp_ -s 1 -c 1`.
+
+  python profiles/prof_bp.py [mixed|fp32|fp32_exact] [n_batches]
+"""
+import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import torch  # noqa: E402
+
+import fdk_b200 as F  # noqa: E402
+from fdk_b200 import phantom as P  # noqa: E402
+
+prec = sys.argv[1] if len(sys.argv) > 1 else "mixed"
+nb = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+p = F.config("c2")
+views = torch.empty((32 * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
+P.project(p, P.phantom_for(p, 2, 20), 0, 32 * nb, views.data_ptr())
+r = F.Reconstructor(p, prec, batch=32)
+for b in range(nb):
+    r.push_device(views[32 * b:].data_ptr(), 32 * b, 32)
+r.sync()
+print(prec, r.stats())
