@@ -13,6 +13,7 @@
 
 #include "bp_exact.cuh"
 #include "bp_fast.cuh"
+#include "bp_tma.cuh"
 #include "common.h"
 
 namespace fdk {
@@ -186,8 +187,9 @@ int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
 // Backproject n views already resident on the device.
 //   layout TRANSPOSED: f32 frames of proj_h rows x proj_w (the reference's BP input)
 //   layout MIRROR: mirror pairs (f32x2 or f16x2 per precision), proj_h rows x proj_w pairs
-int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const float *d_mats, int n,
-              int width, int height, cudaStream_t st, const float *acc_scale = nullptr) {
+int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const float *d_mats,
+              const float *host_mats, int n, int width, int height, cudaStream_t st,
+              const float *acc_scale = nullptr) {
     std::pair<cudaEvent_t, cudaEvent_t> tm;
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
@@ -217,11 +219,34 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
         FDK_CUDA(cudaGetLastError());
     } else {
         FDK_CHECK_ARG(layout == FDK_LAYOUT_MIRROR, "fast backprojection reads the MIRROR layout");
-        FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, 1.0e6f, acc_scale));
+        if (h->plan.tma_ok && ((uintptr_t)dev_proj & 15) == 0) {
+            if (h->precision == FDK_BP_MIXED)
+                FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
+                                               acc_scale));
+            else
+                FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
+                                              acc_scale));
+        } else {
+            const float ws = weight_scale(host_mats, h->top.x + 0.5f * (h->top.width - 1),
+                                          h->top.y + 0.5f * (h->top.height - 1));
+            FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, ws, acc_scale));
+        }
     }
     FDK_CUDA(cudaEventRecord(tm.second, st));
     h->timers.push_back(tm);
     h->bp_count += n;
+    return FDK_OK;
+}
+
+// The TMA kernel's bounded waits report through a device error word; read it after a sync.
+int check_device_error(fdk_bp *h) {
+    if (!h->plan.d_err) return FDK_OK;
+    unsigned int e = 0;
+    FDK_CUDA(cudaMemcpy(&e, h->plan.d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) {
+        cudaMemset(h->plan.d_err, 0, sizeof(e));
+        return fail(FDK_ERR_DEVICE_CHECK, "backprojection pipeline wait timed out on the device (error word %u)", e);
+    }
     return FDK_OK;
 }
 
@@ -252,6 +277,8 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
     FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
     const fdk_box t = *sub_top, b = *sub_bottom;
     FDK_CHECK_ARG(t.width > 0 && t.height > 0 && t.depth > 0, "empty top box");
+    FDK_CHECK_ARG(precision == FDK_BP_FP32_EXACT || b.depth > 0,
+                  "the staged backprojection kernels need the mirror slab pair (subBottom.depth > 0)");
     FDK_CHECK_ARG(t.x + t.width <= (uint64_t)nx && t.y + t.height <= (uint64_t)ny && t.z + t.depth <= (uint64_t)nz,
                   "top box outside the volume");
     const bool sym = b.depth > 0;
@@ -301,10 +328,20 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             ck(cudaMalloc(&h->d_comp, sizeof(float) * nvox), "compensation");
             if (s == FDK_OK) ck(cudaMemset(h->d_comp, 0, sizeof(float) * nvox), "compensation zero");
         }
-        if (s == FDK_OK) {
-            FDK_CHECK_ARG(sym, "the fast backprojection kernels need the mirror slab pair (subBottom.depth > 0)");
+        if (s == FDK_OK)
             s = bp_fast_plan(h->plan, precision, proj_width, proj_height, (int)t.x, (int)t.y, (int)t.z,
                              (int)t.width, (int)t.height, (int)t.depth, h->D, device);
+        if (s == FDK_OK) {
+            // The TMA kernel needs 16-byte row strides; FDK_BP_KERNEL=staged selects the
+            // synchronous-staging kernel instead (kept for comparison and as the fallback).
+            const char *sel = getenv("FDK_BP_KERNEL");
+            h->plan.tma_ok = ((size_t)proj_width * esz) % 16 == 0 && !(sel && std::string(sel) == "staged");
+            if (h->plan.tma_ok) {
+                s = precision == FDK_BP_MIXED ? tma_prepare<__half2>(h->plan.tma_ctas, device)
+                                              : tma_prepare<float2>(h->plan.tma_ctas, device);
+                if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
+                if (s == FDK_OK) ck(cudaMemset(h->plan.d_err, 0, sizeof(unsigned int)), "error word");
+            }
         }
     }
     if (s != FDK_OK) {
@@ -346,7 +383,7 @@ int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t widt
     FDK_CUDA(cudaStreamWaitEvent(h->stream, h->copied[k], 0));
     if (h->precision == FDK_BP_FP32_EXACT) {
         FDK_TRY(launch_bp(h, h->d_stage[k], transpose ? FDK_LAYOUT_TRANSPOSED : FDK_LAYOUT_ROWS, transpose, d_mats,
-                          n_proj, width, height, h->stream));
+                          proj_mat, n_proj, width, height, h->stream));
     } else {
         const long long total = (long long)frame * n_proj;
         const int blocks = (int)std::min<long long>(ceil_div(total, 256), 148 * 16);
@@ -362,7 +399,7 @@ int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t widt
                                                                     height, n_proj);
         }
         FDK_CUDA(cudaGetLastError());
-        FDK_TRY(launch_bp(h, h->d_mirror, FDK_LAYOUT_MIRROR, 1, d_mats, n_proj, width, height, h->stream,
+        FDK_TRY(launch_bp(h, h->d_mirror, FDK_LAYOUT_MIRROR, 1, d_mats, proj_mat, n_proj, width, height, h->stream,
                           acc_scale));
     }
     FDK_CUDA(cudaEventRecord(h->consumed[k], h->stream));
@@ -386,7 +423,7 @@ int fdk_bp_bp_device(fdk_bp *h, const void *dev_proj, int32_t layout, const floa
     FDK_CUDA(cudaStreamWaitEvent(st, h->consumed[k], 0));
     FDK_CUDA(cudaMemcpyAsync(d_mats, proj_mat, sizeof(float) * 12 * n_proj, cudaMemcpyHostToDevice, st));
     // the matrices come from pageable host memory: the async copy completes before returning
-    FDK_TRY(launch_bp(h, dev_proj, layout, 1, d_mats, n_proj, h->proj_w, h->proj_h, st,
+    FDK_TRY(launch_bp(h, dev_proj, layout, 1, d_mats, proj_mat, n_proj, h->proj_w, h->proj_h, st,
                       h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr));
     FDK_CUDA(cudaEventRecord(h->consumed[k], st));
     return FDK_OK;
@@ -404,6 +441,7 @@ int fdk_bp_get_volume(fdk_bp *h, float *host_vol, int64_t size) {
     FDK_CUDA(cudaStreamSynchronize(h->copy_stream));
     FDK_CUDA(cudaStreamSynchronize(h->stream));
     FDK_CUDA(cudaDeviceSynchronize());  // device-resident launches may use caller streams
+    FDK_TRY(check_device_error(h));
     if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
     return transform_volume_to_host(h->d_vol, (int)h->top.width, (int)h->top.height, h->D, host_vol, h->stream);
     FDK_ABI_END
@@ -415,6 +453,7 @@ int fdk_bp_volume_device(fdk_bp *h, float **dev_vol, int64_t *count) {
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
     FDK_CUDA(cudaDeviceSynchronize());
+    FDK_TRY(check_device_error(h));
     const long long nvox = (long long)h->top.width * h->top.height * h->D;
     if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
     FDK_CUDA(cudaStreamSynchronize(h->stream));
@@ -430,6 +469,7 @@ int fdk_bp_stats(fdk_bp *h, int64_t *bp_count, double *kernel_ms) {
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
     FDK_TRY(collect_timers(h));
+    FDK_TRY(check_device_error(h));
     if (bp_count) *bp_count = h->bp_count;
     if (kernel_ms) *kernel_ms = h->kernel_ms;
     return FDK_OK;
@@ -505,7 +545,7 @@ int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layo
     if (h->precision != FDK_BP_FP32_EXACT) FDK_TRY(check_circular(host_mats, n_proj));
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    return launch_bp(h, dev_proj, layout, 1, dev_mats, n_proj, h->proj_w, h->proj_h, (cudaStream_t)stream,
-                     h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr);
+    return launch_bp(h, dev_proj, layout, 1, dev_mats, host_mats, n_proj, h->proj_w, h->proj_h,
+                     (cudaStream_t)stream, h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr);
     FDK_ABI_END
 }

@@ -44,6 +44,9 @@ struct BpFastPlan {
     long long D = 0;
     int device = 0;
     float *d_scale = nullptr; // device scalar: accumulator scale of the MIXED path
+    bool tma_ok = false;      // the TMA kernel applies (row stride a multiple of 16 B)
+    int tma_ctas = 0;         // persistent grid size of the TMA kernel
+    unsigned int *d_err = nullptr;  // device error word of the TMA kernel
 };
 
 struct BpFastArgs {
@@ -327,7 +330,9 @@ inline int bp_fast_plan(BpFastPlan &p, int precision, int proj_w, int proj_h, in
 
 inline void bp_fast_release(BpFastPlan &p) {
     if (p.d_scale) cudaFree(p.d_scale);
+    if (p.d_err) cudaFree(p.d_err);
     p.d_scale = nullptr;
+    p.d_err = nullptr;
 }
 
 // wscale: 1/w^2 is ~1e-6 for mm geometries; multiplying by the squared source distance of the

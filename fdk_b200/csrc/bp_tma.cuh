@@ -1,0 +1,522 @@
+// bp_tma.cuh -- persistent, TMA-fed voxel-driven backprojection for sm_100a.
+//
+// Same geometry contract, MIRROR view layout and bounds rule as bp_fast.cuh (circular orbit,
+// slab pair, element (u, v) = (P[u][v], P[u][nv-1-v])).  What changes is how views reach
+// shared memory and how the gather is indexed:
+//
+//  * Persistent CTAs walk the (16 x 16 column) x (R slices) tiles, x fastest, so the tiles in
+//    flight at any moment sit in the same z band and share detector rows in L2.
+//  * Warp 8 is the producer.  For each chunk of NV views of the current tile it computes the
+//    detector footprint of the tile's voxels (8 corners; a linear-fractional map takes its
+//    extremes there), and one lane issues a 3-D TMA tile load (cp.async.bulk.tensor) of a
+//    BW x BH element box per view into a ring of S stages, completing on an mbarrier
+//    (expect_tx).  Consumers release a stage through a second mbarrier.  No CTA-wide barrier
+//    is on the hot path, and no consumer instruction is spent on staging.
+//  * Warps 0-7 consume.  Lanes are an 8 x 4 block of voxel columns: their detector samples
+//    fall on about ten box rows at nearly the same v, and a row pitch of BW = 36 words
+//    (4 mod 32) spreads them over the banks (measured model: ~1.2 wavefronts per gather,
+//    against 2.9 for 16 x 2 lanes with pitch 24).
+//  * FP16 path: v is carried in fixed point, t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per
+//    voxel.  The integer part of t's bits indexes the box; the low 10 bits are the fraction,
+//    which OR-ed under the FP16 exponent of 1.0 gives 1 + fv as a half directly.  The two
+//    u-lerps use weights (1-fu) w and fu w folded in, the v-lerp is one HFMA2 over the
+//    (voxel, mirror) pair, and the result is added to FP32 accumulators with the sm_100
+//    mixed-precision add (add.rn.f32.f16).
+//
+// Every wait is bounded (kWaitLimit polls); a timeout sets the device error word, the CTA
+// drains the copies it issued (bounded) and returns.
+#pragma once
+#include <cuda.h>
+#include <cuda_fp16.h>
+
+#include "common.h"
+
+namespace fdk {
+
+template <typename E>
+struct TmaCfg;
+template <>
+struct TmaCfg<__half2> {
+    static constexpr int R = 12;   // top-slab slices per thread
+    static constexpr int BW = 36;  // box width (v elements), 144 B rows
+    static constexpr int BH = 40;  // box height (u rows)
+    static constexpr int NV = 4;   // views per stage
+    static constexpr int S = 3;    // stages
+};
+template <>
+struct TmaCfg<float2> {
+    static constexpr int R = 8;
+    static constexpr int BW = 34;  // 272 B rows
+    static constexpr int BH = 40;
+    static constexpr int NV = 4;
+    static constexpr int S = 2;
+};
+
+constexpr long long kWaitLimit = 1ll << 26;
+constexpr unsigned long long kWaitNs = 10ull * 1000 * 1000 * 1000;  // 10 s
+constexpr unsigned kErrTimeout = 1u;
+
+struct __align__(16) TmaMeta {
+    float m[12];
+    int u_lo, v_lo, staged, interior;
+};
+
+struct BpTmaArgs {
+    float *vol;
+    float *comp;
+    const void *proj;    // MIRROR layout (global gathers of views that do not fit the box)
+    const float *mats;   // 12 floats per view (device)
+    const float *scale;  // accumulator scale (device scalar) or null
+    unsigned int *err;   // device error word
+    int n_proj, nu, nv;
+    int x0, y0, z0, nxs, nys, nzz;
+    long long D;
+    float wscale;
+    int tiles_x, tiles_y, tiles_z;
+};
+
+template <typename E>
+__host__ __device__ constexpr int tma_box_bytes() {
+    return ((TmaCfg<E>::BW * TmaCfg<E>::BH * (int)sizeof(E)) + 127) / 128 * 128;
+}
+template <typename E>
+__host__ __device__ constexpr int tma_smem_bytes() {
+    return TmaCfg<E>::S * TmaCfg<E>::NV * (tma_box_bytes<E>() + (int)sizeof(TmaMeta)) + 2 * TmaCfg<E>::S * 8;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait for the phase with the given parity: gives up after kWaitNs of wall time (or
+// kWaitLimit polls); false on timeout.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+    unsigned long long t0 = 0;
+    for (long long i = 0; i < kWaitLimit; i++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((i & 255) == 0) {
+            const unsigned long long t = global_ns();
+            if (i == 0) t0 = t;
+            else if (t - t0 > kWaitNs) return false;
+        }
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ unsigned lds32(unsigned addr) {
+    unsigned v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ float2 lds64f(unsigned addr) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ __half2 u2h(unsigned u) { return *reinterpret_cast<__half2 *>(&u); }
+__device__ __forceinline__ void acc_add_f16x2(float &lo_acc, float &hi_acc, __half2 r) {
+    const unsigned u = *reinterpret_cast<unsigned *>(&r);
+    asm("{\n .reg .f16 lo, hi;\n mov.b32 {lo, hi}, %2;\n add.rn.f32.f16 %0, lo, %0;\n add.rn.f32.f16 %1, hi, %1;\n}"
+        : "+f"(lo_acc), "+f"(hi_acc)
+        : "r"(u));
+}
+
+// Footprint box of a tile in one view; fills meta (matrix copied by the caller).
+template <typename E>
+__device__ __forceinline__ void tile_box(const float *m, float xa, float xb, float ya, float yb, float za, float zb,
+                                         int nu, int nv, TmaMeta &md) {
+    using C = TmaCfg<E>;
+    float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        const float x = (c & 1) ? xb : xa, y = (c & 2) ? yb : ya;
+        const float rw = 1.0f / fmaf(m[8], x, fmaf(m[9], y, m[11]));
+        const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
+        const float vw = fmaf(m[4], x, fmaf(m[5], y, m[7]));
+        const float va = fmaf(m[6], za, vw) * rw, vb = fmaf(m[6], zb, vw) * rw;
+        umin = fminf(umin, U);
+        umax = fmaxf(umax, U);
+        vmin = fminf(vmin, fminf(va, vb));
+        vmax = fmaxf(vmax, fmaxf(va, vb));
+    }
+    // one element of margin absorbs FP32 differences between corners and per-column math
+    const float ulo = fmaxf(floorf(umin) - 1.f, -1.f), uhi = fminf(floorf(umax) + 2.f, (float)nu);
+    const float vlo = fmaxf(floorf(vmin) - 1.f, -8.f), vhi = fminf(floorf(vmax) + 2.f, (float)nv + 4.f);
+    const int u_lo = (int)ulo;
+    const int v_lo = ((int)vlo) & ~3;  // 16-byte aligned TMA x coordinate (floor for negatives)
+    md.u_lo = u_lo;
+    md.v_lo = v_lo;
+    md.staged = ((int)uhi - u_lo + 1 <= C::BH && (int)vhi - v_lo + 1 <= C::BW) ? 1 : 0;
+    md.interior = (umin >= 0.f && umax < (float)(nu - 1) - 1e-3f && vmin > 1e-3f && vmax < (float)(nv - 1) - 1e-3f)
+                      ? 1
+                      : 0;
+}
+
+// One view's contribution to a thread's column: R voxel pairs.
+template <typename E>
+__device__ __forceinline__ void column_view(const TmaMeta &md, unsigned box, const E *gview, float x, float y,
+                                            float zf0, int nu, int nv, float wscale, float (&am)[TmaCfg<E>::R],
+                                            float (&ar)[TmaCfg<E>::R]) {
+    using C = TmaCfg<E>;
+    constexpr int R = C::R;
+    const float *m = md.m;
+    const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
+    const float rw = __frcp_rn(w);
+    const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
+    const float A = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], zf0, m[7]))) * rw;  // v at the run's first slice
+    const float B = m[6] * rw;                                                  // dv per slice
+    const float wt = rw * rw * wscale;
+    if (!(U >= 0.f && U < (float)(nu - 1))) return;  // every sample of this column is zero
+    const float fuf = floorf(U);
+    const float fu = U - fuf;
+    const int u0 = (int)fuf;
+
+    if constexpr (sizeof(E) == 4) {
+        const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
+        if (md.staged && md.interior) {
+            // fixed point: t = (v - v_lo) * 1024 + 1.5 * 2^23; bits = 0x4B400000 + round(1024 (v - v_lo))
+            const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
+            const float B1 = B * 1024.f;
+            const unsigned rowp = box + (unsigned)((u0 - md.u_lo) * C::BW * 4) - (0x4B400000u >> 10) * 4u;
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+                const unsigned a = rowp + (bits >> 10) * 4u;
+                const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
+                const __half2 e0 = u2h(lds32(a)), e1 = u2h(lds32(a + 4));
+                const __half2 e2 = u2h(lds32(a + C::BW * 4)), e3 = u2h(lds32(a + C::BW * 4 + 4));
+                const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
+                const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
+                const __half2 d = __hsub2(c1, c0);
+                const __half2 r = __hfma2(fvh, d, __hsub2(c0, d));
+                acc_add_f16x2(am[k], ar[k], r);
+            }
+            return;
+        }
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const float v = fmaf(B, (float)k, A);
+            const float vr = (float)(nv - 1) - v;
+            const bool mv = v >= 0.f && v < (float)(nv - 1);
+            const bool rv = vr >= 0.f && vr < (float)(nv - 1);
+            if (!(mv || rv)) continue;
+            const float vf = fminf(floorf(v), (float)(nv - 2));
+            const int vi = (int)vf;
+            const __half2 fv2 = __float2half2_rn(v - vf);
+            __half2 e0, e1, e2, e3;
+            if (md.staged) {
+                const unsigned a = box + (unsigned)(((u0 - md.u_lo) * C::BW + (vi - md.v_lo)) * 4);
+                e0 = u2h(lds32(a));
+                e1 = u2h(lds32(a + 4));
+                e2 = u2h(lds32(a + C::BW * 4));
+                e3 = u2h(lds32(a + C::BW * 4 + 4));
+            } else {
+                const unsigned *g0 = reinterpret_cast<const unsigned *>(gview) + (long long)u0 * nv + vi;
+                e0 = u2h(__ldg(g0));
+                e1 = u2h(__ldg(g0 + 1));
+                e2 = u2h(__ldg(g0 + nv));
+                e3 = u2h(__ldg(g0 + nv + 1));
+            }
+            const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
+            const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
+            __half2 r = __hfma2(fv2, __hsub2(c1, c0), c0);
+            const float2 rf = __half22float2(r);
+            if (mv) am[k] += rf.x;
+            if (rv) ar[k] += rf.y;
+        }
+    } else {
+        const float wa = (1.f - fu) * wt, wb = fu * wt;
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const float v = fmaf(B, (float)k, A);
+            bool mv = true, rv = true;
+            float vf;
+            if (!(md.staged && md.interior)) {
+                const float vr = (float)(nv - 1) - v;
+                mv = v >= 0.f && v < (float)(nv - 1);
+                rv = vr >= 0.f && vr < (float)(nv - 1);
+                if (!(mv || rv)) continue;
+                vf = fminf(floorf(v), (float)(nv - 2));
+            } else {
+                vf = floorf(v);
+            }
+            const int vi = (int)vf;
+            const float fv = v - vf;
+            float2 e0, e1, e2, e3;
+            if (md.staged) {
+                const unsigned a = box + (unsigned)(((u0 - md.u_lo) * C::BW + (vi - md.v_lo)) * 8);
+                e0 = lds64f(a);
+                e1 = lds64f(a + 8);
+                e2 = lds64f(a + C::BW * 8);
+                e3 = lds64f(a + C::BW * 8 + 8);
+            } else {
+                const float2 *g0 = reinterpret_cast<const float2 *>(gview) + (long long)u0 * nv + vi;
+                e0 = __ldg(g0);
+                e1 = __ldg(g0 + 1);
+                e2 = __ldg(g0 + nv);
+                e3 = __ldg(g0 + nv + 1);
+            }
+            const float c0x = fmaf(e2.x, wb, e0.x * wa), c0y = fmaf(e2.y, wb, e0.y * wa);
+            const float c1x = fmaf(e3.x, wb, e1.x * wa), c1y = fmaf(e3.y, wb, e1.y * wa);
+            if (mv) am[k] += fmaf(fv, c1x - c0x, c0x);
+            if (rv) ar[k] += fmaf(fv, c1y - c0y, c0y);
+        }
+    }
+}
+
+template <typename E>
+__global__ void __launch_bounds__(288, 1) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
+    using C = TmaCfg<E>;
+    constexpr int R = C::R, NV = C::NV, S = C::S;
+    constexpr int BOX = tma_box_bytes<E>();
+    constexpr unsigned BOX_TX = C::BW * C::BH * sizeof(E);
+    extern __shared__ __align__(128) unsigned char smem[];
+    TmaMeta *meta = reinterpret_cast<TmaMeta *>(smem + S * NV * BOX);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(meta + S * NV);
+    const unsigned boxes = smem_u32(smem);
+    const unsigned full0 = smem_u32(bars), empty0 = smem_u32(bars + S);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 8);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int n_chunks = (a.n_proj + NV - 1) / NV;
+    const int n_tiles = a.tiles_x * a.tiles_y * a.tiles_z;
+    const long long frame = (long long)a.nu * a.nv;
+
+    if (warp == 8) {
+        // ---------------- producer
+        int it = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+            const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y, tz = tile / (a.tiles_x * a.tiles_y);
+            const float xa = (float)(a.x0 + tx * 16), xb = (float)(a.x0 + min(tx * 16 + 16, a.nxs) - 1);
+            const float ya = (float)(a.y0 + ty * 16), yb = (float)(a.y0 + min(ty * 16 + 16, a.nys) - 1);
+            const float za = (float)(a.z0 + tz * R), zb = za + (float)(R - 1);
+            for (int c = 0; c < n_chunks; c++, it++) {
+                const int s = it % S;
+                const unsigned ph = (unsigned)(it / S) & 1u;
+                if (it >= S && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                    ok = false;
+                    break;
+                }
+                const int view = c * NV + lane;
+                if (lane < NV) {
+                    TmaMeta &md = meta[s * NV + lane];
+                    if (view < a.n_proj) {
+#pragma unroll
+                        for (int q = 0; q < 12; q++) md.m[q] = __ldg(a.mats + 12 * view + q);
+                        tile_box<E>(md.m, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
+                    } else {
+                        md.staged = 0;
+                        md.interior = 0;
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    unsigned n_staged = 0;
+                    for (int l = 0; l < NV; l++)
+                        if (c * NV + l < a.n_proj && meta[s * NV + l].staged) n_staged++;
+                    mbar_arrive_tx(full0 + 8 * s, n_staged * BOX_TX);
+                    for (int l = 0; l < NV; l++) {
+                        const TmaMeta &md = meta[s * NV + l];
+                        if (c * NV + l < a.n_proj && md.staged)
+                            tma_load_3d(boxes + (s * NV + l) * BOX, &tmap, md.v_lo, md.u_lo, c * NV + l, full0 + 8 * s);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        if (!ok) {
+            if (lane == 0) atomicOr(a.err, kErrTimeout);
+            // drain: wait (bounded) for the stages whose copies may still be in flight
+            if (lane == 0)
+                for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(full0 + 8 * (k % S), (unsigned)(k / S) & 1u);
+        }
+        return;
+    }
+
+    // ---------------- consumers: warps 0..7, lanes = 8 x 4 columns
+    const int wx = warp & 1, wy = warp >> 1;
+    const int lx = lane & 7, ly = lane >> 3;
+    const E *proj = reinterpret_cast<const E *>(a.proj);
+    int it = 0;
+    for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y, tz = tile / (a.tiles_x * a.tiles_y);
+        const int xi = tx * 16 + wx * 8 + lx, yi = ty * 16 + wy * 4 + ly;
+        const bool col_ok = xi < a.nxs && yi < a.nys;
+        const float x = (float)(a.x0 + xi), y = (float)(a.y0 + yi);
+        const int zt = tz * R;
+        const float zf0 = (float)(a.z0 + zt);
+        float am[R], ar[R];
+#pragma unroll
+        for (int k = 0; k < R; k++) am[k] = ar[k] = 0.f;
+        for (int c = 0; c < n_chunks; c++, it++) {
+            const int s = it % S;
+            const unsigned ph = (unsigned)(it / S) & 1u;
+            if (!mbar_wait(full0 + 8 * s, ph)) {
+                if (lane == 0) atomicOr(a.err, kErrTimeout);
+                return;
+            }
+            if (col_ok) {
+                for (int l = 0; l < NV; l++) {
+                    const int view = c * NV + l;
+                    if (view >= a.n_proj) break;
+                    column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + view * frame, x, y, zf0, a.nu,
+                                   a.nv, a.wscale, am, ar);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(empty0 + 8 * s);
+        }
+        if (col_ok) {
+            const float sc = (a.scale ? *a.scale : 1.0f) / a.wscale;
+            float *out = a.vol + ((long long)xi * a.nys + yi) * a.D;
+            float *cmp = a.comp ? a.comp + ((long long)xi * a.nys + yi) * a.D : nullptr;
+            const int nrun = min(R, a.nzz - zt);
+#pragma unroll
+            for (int k = 0; k < R; k++) {  // static indices keep the accumulators in registers
+                if (k >= nrun) break;
+                const long long i1 = zt + k, i2 = a.D - 1 - i1;
+                const float dm = am[k] * sc, dr = ar[k] * sc;
+                if (cmp) {
+                    const float y1 = dm - cmp[i1], t1 = out[i1] + y1;
+                    cmp[i1] = (t1 - out[i1]) - y1;
+                    out[i1] = t1;
+                    const float y2 = dr - cmp[i2], t2 = out[i2] + y2;
+                    cmp[i2] = (t2 - out[i2]) - y2;
+                    out[i2] = t2;
+                } else {
+                    out[i1] += dm;
+                    out[i2] += dr;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace fdk
+
+// ---------------------------------------------------------------------------------------
+// host side
+namespace fdk {
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link, so the
+// library still loads on machines without a driver).
+inline EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 3-D map over MIRROR views [n][nu][nv] of esz-byte elements, box BW x BH x 1, zero fill.
+template <typename E>
+inline int encode_views_map(CUtensorMap *map, const void *base, int nu, int nv, int n) {
+    EncodeTiledFn enc = tensor_map_encoder();
+    if (!enc) return fail(FDK_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[3] = {(cuuint64_t)nv, (cuuint64_t)nu, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)nv * sizeof(E), (cuuint64_t)nu * nv * sizeof(E)};
+    const cuuint32_t box[3] = {(cuuint32_t)TmaCfg<E>::BW, (cuuint32_t)TmaCfg<E>::BH, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = sizeof(E) == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    CUresult r = enc(map, dt, 3, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(FDK_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return FDK_OK;
+}
+
+template <typename E>
+inline int tma_prepare(int &ctas, int device) {
+    const int smem = tma_smem_bytes<E>();
+    FDK_CUDA(cudaFuncSetAttribute(bp_tma_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0, sms = 0;
+    FDK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_tma_kernel<E>, 288, smem));
+    FDK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    ctas = sms * (per_sm > 0 ? per_sm : 1);
+    return FDK_OK;
+}
+
+// Square of the source distance of the volume centre in view 0: keeps f^2 * wscale near 1.
+inline float weight_scale(const float *host_mats, float xc, float yc) {
+    const float w = host_mats[8] * xc + host_mats[9] * yc + host_mats[11];
+    return (w > 0.f) ? w * w : 1.0f;
+}
+
+template <typename E>
+inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const void *proj, const float *d_mats,
+                         const float *host_mats, int n, cudaStream_t st, const float *scale) {
+    using C = TmaCfg<E>;
+    FDK_CHECK_ARG(((uintptr_t)proj & 15) == 0, "TMA views must start on a 16-byte boundary");
+    CUtensorMap map;
+    FDK_TRY(encode_views_map<E>(&map, proj, p.nu, p.nv, n));
+    BpTmaArgs a;
+    a.vol = vol;
+    a.comp = comp;
+    a.proj = proj;
+    a.mats = d_mats;
+    a.scale = scale;
+    a.err = p.d_err;
+    a.n_proj = n;
+    a.nu = p.nu;
+    a.nv = p.nv;
+    a.x0 = p.x0;
+    a.y0 = p.y0;
+    a.z0 = p.z0;
+    a.nxs = p.nxs;
+    a.nys = p.nys;
+    a.nzz = p.nzz;
+    a.D = p.D;
+    a.wscale = weight_scale(host_mats, p.x0 + 0.5f * (p.nxs - 1), p.y0 + 0.5f * (p.nys - 1));
+    a.tiles_x = (int)ceil_div(p.nxs, 16);
+    a.tiles_y = (int)ceil_div(p.nys, 16);
+    a.tiles_z = (int)ceil_div(p.nzz, C::R);
+    const long long n_tiles = (long long)a.tiles_x * a.tiles_y * a.tiles_z;
+    FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
+    const int grid = (int)std::min<long long>(n_tiles, p.tma_ctas);
+    bp_tma_kernel<E><<<grid, 288, tma_smem_bytes<E>(), st>>>(map, a);
+    FDK_CUDA(cudaGetLastError());
+    return FDK_OK;
+}
+
+}  // namespace fdk

@@ -96,9 +96,13 @@ def test_exact_bitwise_vs_reference_kernel(views):
     assert np.array_equal(ref, oracle_bp_ref32(top, bot[5], n, batches, mb))  # pins the oracle
 
 
+@pytest.mark.parametrize("kernel", ["tma", "staged"])
 @pytest.mark.parametrize("precision,tol", [("fp32", 1e-5), ("mixed", 1e-3)])
-@pytest.mark.parametrize("n,views", [(32, 24), (64, 64)])
-def test_fast_paths_on_phantom(precision, tol, n, views):
+@pytest.mark.parametrize("n,views", [(32, 24), (64, 64), (96, 40)])
+def test_fast_paths_on_phantom(precision, tol, n, views, kernel, monkeypatch):
+    """Both staged kernels: the TMA-fed persistent kernel and the synchronous-staging one."""
+    if kernel == "staged":
+        monkeypatch.setenv("FDK_BP_KERNEL", "staged")
     p = small_param(n, n, n, views)
     mats = p.proj_matrices()
     _, proj = phantom_views(p, seed=n)
@@ -118,18 +122,23 @@ def test_fast_paths_on_phantom(precision, tol, n, views):
     assert e64 <= tol
 
 
-def test_fast_fp32_border_views():
+@pytest.mark.parametrize("kernel", ["tma", "staged"])
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+@pytest.mark.parametrize("nu,nv", [(24, 20), (26, 21)])  # nv=21: rows not 16-byte multiples
+def test_fast_border_views(precision, kernel, nu, nv, monkeypatch):
     """Detector smaller than the volume's shadow: boundary samples follow SUBPIXEL's rule."""
+    if kernel == "staged":
+        monkeypatch.setenv("FDK_BP_KERNEL", "staged")
     n, views = 32, 16
-    p = small_param(n, 24, 20, views)  # detector crops the volume in u and v
+    p = small_param(n, nu, nv, views)  # detector crops the volume in u and v
     p.du = p.dv = 384.0 / 40
     mats = p.proj_matrices()
-    filt = random_views(views, 24, 20, seed=21)
+    filt = random_views(views, nu, nv, seed=21)
     top = [0, 0, 0, n, n, n // 2]
     bot = [0, 0, n // 2, n, n, n // 2]
-    got = run_bp("fp32", p, top, bot, [filt], [mats])
+    got = run_bp(precision, p, top, bot, [filt], [mats])
     want = oracle_bp_ref32(top, bot[5], n, [filt], [mats])
-    assert rel_l2(got, want) <= 1e-5, rel_l2(got, want)
+    assert rel_l2(got, want) <= (1e-5 if precision == "fp32" else 1e-3), rel_l2(got, want)
 
 
 def test_fast_rejects_non_circular_matrices():
