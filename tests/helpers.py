@@ -60,3 +60,26 @@ def oracle_bp_f64(top, depth_bottom, nz, filt, mats64):
     vol = np.zeros(top[3] * top[4] * D, np.float64)
     O.bp_f64(vol, top, depth_bottom, nz, filt, mats64)
     return O.transform_volume(vol.astype(np.float32), top[3], top[4], D), vol
+
+
+def knife_edge_mask(p, top, depth_bottom, eps=1e-3):
+    """Voxels (in [zs][y][x] storage order of the slab pair) whose projection in some view
+    lands within eps pixels of a detector border (u or v at 0 or n-1).  The reference's
+    bilinear rule (backprojectionFDK.cu:18) zeroes a sample at u, v >= n-1 and keeps it just
+    below, so at the border any change of FP32 rounding switches a whole sample on or off.
+    Parity between different FP32 arithmetics is measured on the other voxels."""
+    mats = p.proj_matrices(np.float64)
+    D = top[5] + depth_bottom
+    zs = np.concatenate([np.arange(top[2], top[2] + top[5]),
+                         np.arange(p.nz - top[2] - depth_bottom, p.nz - top[2])]) if depth_bottom else \
+        np.arange(top[2], top[2] + top[5])
+    z, y, x = np.meshgrid(zs.astype(np.float64), np.arange(top[1], top[1] + top[4], dtype=np.float64),
+                          np.arange(top[0], top[0] + top[3], dtype=np.float64), indexing="ij")
+    bad = np.zeros(z.shape, bool)
+    for m in mats:
+        w = m[8] * x + m[9] * y + m[10] * z + m[11]
+        u = (m[0] * x + m[1] * y + m[2] * z + m[3]) / w
+        v = (m[4] * x + m[5] * y + m[6] * z + m[7]) / w
+        for c, n in ((u, p.nu), (v, p.nv)):
+            bad |= (np.abs(c) < eps) | (np.abs(c - (n - 1)) < eps)
+    return ~bad
