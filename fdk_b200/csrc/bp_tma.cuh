@@ -185,7 +185,7 @@ __device__ __forceinline__ void column_view(const TmaMeta &md, unsigned box, con
     constexpr int R = C::R;
     const float *m = md.m;
     const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
-    const float rw = __frcp_rn(w);
+    const float rw = __fdividef(1.0f, w);
     const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
     const float A = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], zf0, m[7]))) * rw;  // v at the run's first slice
     const float B = m[6] * rw;                                                  // dv per slice
@@ -288,8 +288,92 @@ __device__ __forceinline__ void column_view(const TmaMeta &md, unsigned box, con
     }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Prefetch a thread's two volume segments (top run and mirror run, and their compensation
+// terms) into L2 at the start of a tile, so the write-back at its end does not wait on DRAM.
+template <int R>
+__device__ __forceinline__ void prefetch_column(const float *vol, const float *comp, long long base, long long D,
+                                                int zt) {
+    const long long t0 = base + zt, b0 = base + D - zt - R;
+    prefetch_l2(vol + t0);
+    prefetch_l2(vol + t0 + R - 1);
+    prefetch_l2(vol + b0);
+    prefetch_l2(vol + b0 + R - 1);
+    if (comp) {
+        prefetch_l2(comp + t0);
+        prefetch_l2(comp + t0 + R - 1);
+        prefetch_l2(comp + b0);
+        prefetch_l2(comp + b0 + R - 1);
+    }
+}
+
+// Add a thread's accumulators to its column: top slices zt..zt+nrun-1 and their mirrors
+// D-1-zt-k.  Loads are issued before any store (restrict pointers), as 128-bit accesses when
+// the runs are 16-byte aligned; with comp, a compensated (Kahan) sum across launches.
+template <int R>
+__device__ __forceinline__ void write_back(float *__restrict__ vol, float *__restrict__ comp, long long base,
+                                           long long D, int zt, int nrun, float sc, const float (&am)[R],
+                                           const float (&ar)[R]) {
+    float *vt = vol + base + zt;           // top run, ascending in k
+    float *vb = vol + base + D - zt - R;   // mirror run: element j holds k = R-1-j
+    float *ct = comp ? comp + base + zt : nullptr;
+    float *cb = comp ? comp + base + D - zt - R : nullptr;
+    if (nrun == R && (R % 4) == 0 && (D % 4) == 0 && (zt % 4) == 0 && ((base & 3) == 0)) {
+        // top run, then mirror run (keeps at most 2R extra values live)
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            float *v = half ? vb : vt;
+            float *c = half ? cb : ct;
+            float t[R], tc[R];
+#pragma unroll
+            for (int q = 0; q < R / 4; q++) {
+                *reinterpret_cast<float4 *>(&t[4 * q]) = reinterpret_cast<const float4 *>(v)[q];
+                if (comp) *reinterpret_cast<float4 *>(&tc[4 * q]) = reinterpret_cast<const float4 *>(c)[q];
+            }
+#pragma unroll
+            for (int k = 0; k < R; k++) {
+                const float d = (half ? ar[R - 1 - k] : am[k]) * sc;  // mirror element k is voxel R-1-k
+                if (comp) {
+                    const float y = d - tc[k], s = t[k] + y;
+                    tc[k] = (s - t[k]) - y;
+                    t[k] = s;
+                } else {
+                    t[k] += d;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < R / 4; q++) {
+                reinterpret_cast<float4 *>(v)[q] = *reinterpret_cast<const float4 *>(&t[4 * q]);
+                if (comp) reinterpret_cast<float4 *>(c)[q] = *reinterpret_cast<const float4 *>(&tc[4 * q]);
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < R; k++) {  // static indices keep the accumulators in registers
+        if (k >= nrun) break;
+        const long long i1 = base + zt + k, i2 = base + D - 1 - zt - k;
+        const float dm = am[k] * sc, dr = ar[k] * sc;
+        if (comp) {
+            const float o1 = vol[i1], c1 = comp[i1], o2 = vol[i2], c2 = comp[i2];
+            const float y1 = dm - c1, s1 = o1 + y1;
+            const float y2 = dr - c2, s2 = o2 + y2;
+            comp[i1] = (s1 - o1) - y1;
+            vol[i1] = s1;
+            comp[i2] = (s2 - o2) - y2;
+            vol[i2] = s2;
+        } else {
+            vol[i1] += dm;
+            vol[i2] += dr;
+        }
+    }
+}
+
 template <typename E>
-__global__ void __launch_bounds__(288, 1) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
+__global__ void __launch_bounds__(288, 2) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
     using C = TmaCfg<E>;
     constexpr int R = C::R, NV = C::NV, S = C::S;
     constexpr int BOX = tma_box_bytes<E>();
@@ -378,6 +462,7 @@ __global__ void __launch_bounds__(288, 1) bp_tma_kernel(const __grid_constant__ 
         const float x = (float)(a.x0 + xi), y = (float)(a.y0 + yi);
         const int zt = tz * R;
         const float zf0 = (float)(a.z0 + zt);
+        if (col_ok) prefetch_column<R>(a.vol, a.comp, ((long long)xi * a.nys + yi) * a.D, a.D, zt);
         float am[R], ar[R];
 #pragma unroll
         for (int k = 0; k < R; k++) am[k] = ar[k] = 0.f;
@@ -401,26 +486,8 @@ __global__ void __launch_bounds__(288, 1) bp_tma_kernel(const __grid_constant__ 
         }
         if (col_ok) {
             const float sc = (a.scale ? *a.scale : 1.0f) / a.wscale;
-            float *out = a.vol + ((long long)xi * a.nys + yi) * a.D;
-            float *cmp = a.comp ? a.comp + ((long long)xi * a.nys + yi) * a.D : nullptr;
-            const int nrun = min(R, a.nzz - zt);
-#pragma unroll
-            for (int k = 0; k < R; k++) {  // static indices keep the accumulators in registers
-                if (k >= nrun) break;
-                const long long i1 = zt + k, i2 = a.D - 1 - i1;
-                const float dm = am[k] * sc, dr = ar[k] * sc;
-                if (cmp) {
-                    const float y1 = dm - cmp[i1], t1 = out[i1] + y1;
-                    cmp[i1] = (t1 - out[i1]) - y1;
-                    out[i1] = t1;
-                    const float y2 = dr - cmp[i2], t2 = out[i2] + y2;
-                    cmp[i2] = (t2 - out[i2]) - y2;
-                    out[i2] = t2;
-                } else {
-                    out[i1] += dm;
-                    out[i2] += dr;
-                }
-            }
+            write_back<R>(a.vol, a.comp, ((long long)xi * a.nys + yi) * a.D, a.D, zt, min(R, a.nzz - zt), sc, am,
+                          ar);
         }
     }
 }
