@@ -1,7 +1,8 @@
-"""Profiling driver (runs committed files only): a few backprojection launches at the 512^3 / 512^2 configuration (views and
-volume larger than L2, a few GB on the device), for `ncu --set full -k regex:bp_ -s 1 -c 1`.
+"""Profiling driver: a few filter + backprojection launches at the 512^3 / 512 x 512 x 512-view
+configuration (views and volume larger than L2, a few GB on the device), small enough for
+`ncu --set full -k regex:bp_ -s 1 -c 1`.
 
-  python profiles/prof_bp.py [mixed|fp32|fp32_exact] [n_batches]
+  python -m fdk_b200.profile_bp [mixed|fp32|fp32_exact] [n_batches]
 """
 import os
 import sys
