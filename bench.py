@@ -370,9 +370,9 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         except Exception:
             hbm_peak, hbm_src = 6650.0, "fallback"
         bp_launch_ms = bp_ms / args.steps
-        traffic = read_traffic(f"bp_{args.precision}_c3.md")
+        traffic = read_traffic(f"bp_tma_{args.precision}_c2.md")
         roofline = {
-            "kernel": f"bp_fast_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
+            "kernel": f"bp_tma_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
             if args.precision != "fp32_exact" else "bp_exact_kernel",
             "bound": "smem" if peak_smem <= peak_fma else "fp32",
             "achieved": kernel_gups, "peak": peak, "unit": "GUPS", "frac": kernel_gups / peak,
@@ -391,7 +391,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
                        "achieved": flt_bytes / (flt_ms / args.steps * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                        "frac": flt_bytes / (flt_ms / args.steps * 1e-3) / 1e9 / hbm_peak,
                        "algorithmic_bytes_per_launch": flt_bytes, "launch_ms": flt_ms / args.steps,
-                       "traffic": read_traffic(f"filter_{args.precision}_c3.md")}
+                       "traffic": read_traffic(f"filter_{args.precision}_c2.md")}
         out = {
             "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
