@@ -36,7 +36,7 @@ EXPORTED = [
     "fdk_geometry_default", "fdk_filter_length", "fdk_filter_design", "fdk_angular_ramp_factor",
     "fdk_cos_table", "fdk_view_angles", "fdk_projection_matrices",
     "fdk_filter_create", "fdk_filter_filtering", "fdk_filter_run_device", "fdk_filter_destroy",
-    "fdk_correct_image_real32", "fdk_filter_row_real32",
+    "fdk_correct_image_real32", "fdk_filter_row_real32", "fdk_filter_row_real32_noalloc",
     "fdk_bp_create", "fdk_bp_bp", "fdk_bp_bp_device", "fdk_bp_get_volume", "fdk_bp_volume_device",
     "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
     "fdk_rtk_reconstruct_conebeam",
@@ -110,6 +110,7 @@ def lib() -> C.CDLL:
         "fdk_filter_destroy": ([vp], C.c_int),
         "fdk_correct_image_real32": ([C.POINTER(DataRef)] * 3, C.c_int),
         "fdk_filter_row_real32": ([C.POINTER(DataRef)] * 3, C.c_int),
+        "fdk_filter_row_real32_noalloc": ([C.POINTER(DataRef)] * 3, C.c_int),
         "fdk_bp_create": ([C.POINTER(vp), i32, i32, i32, i32, i32, i32, C.POINTER(Box), C.POINTER(Box),
                            i32, i32], C.c_int),
         "fdk_bp_bp": ([vp, i32, vp, i32, i32, vp, i32], C.c_int),

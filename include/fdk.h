@@ -140,6 +140,16 @@ typedef struct fdk_dataref {
 } fdk_dataref;
 int fdk_correct_image_real32(const fdk_dataref *src, const fdk_dataref *table, fdk_dataref *dst);
 int fdk_filter_row_real32(const fdk_dataref *src, fdk_dataref *dst, const fdk_dataref *filter);
+/* No counterpart in the reference.  fdk_filter_row_real32 without any device allocation, for
+ * callers that cannot allocate device memory when they filter (they reserve the device budget up
+ * front, or cannot afford cudaMalloc/cudaFree, which may synchronise the device, in their
+ * processing loop).  The FFT tables live in a 32 KiB file-scope device array of the library that
+ * every GPU using the library holds until the process exits; filter->width (W) must be at most
+ * 4096, larger W is rejected with FDK_ERR_INVALID_ARG.  All calls share the array and each call
+ * rewrites the entries it uses; calls that overlap on one GPU (from several host threads) race
+ * and must be serialised by the caller.  The first call on a device looks up the array's address;
+ * make that first call before starting any stream capture.  Synchronous, like the original. */
+int fdk_filter_row_real32_noalloc(const fdk_dataref *src, fdk_dataref *dst, const fdk_dataref *filter);
 
 /* ---- backprojection: BackProjectionFDK (cudaBP/backprojection.cuh:246-271) -- */
 /* Arithmetic of the backprojection kernel.
