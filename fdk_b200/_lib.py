@@ -42,7 +42,9 @@ EXPORTED = [
     "fdk_rtk_reconstruct_conebeam",
     "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device", "fdk_recon_sync",
     "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_reset", "fdk_recon_destroy",
-    "fdk_phantom_project", "fdk_probe_smem", "fdk_probe_fma",
+    "fdk_phantom_project", "fdk_forward_project", "fdk_probe_smem", "fdk_probe_fma",
+    "fdk_nn_param_count", "fdk_nn_forward", "fdk_nn_backward", "fdk_adam_step", "fdk_transmission_noise",
+    "fdk_voxelize", "fdk_rows_to_mirror", "fdk_volume_mse", "fdk_bp_adjoint",
 ]
 
 
@@ -132,6 +134,16 @@ def lib() -> C.CDLL:
         "fdk_recon_reset": ([vp], C.c_int),
         "fdk_recon_destroy": ([vp], C.c_int),
         "fdk_phantom_project": ([G, vp, i32, i64, i64, vp, vp], C.c_int),
+        "fdk_forward_project": ([G, vp, i64, i64, vp, vp], C.c_int),
+        "fdk_nn_param_count": ([], C.c_int),
+        "fdk_nn_forward": ([vp, vp, vp, i64, i32, C.c_float, vp], C.c_int),
+        "fdk_nn_backward": ([vp, vp, vp, vp, i64, i32, C.c_float, vp], C.c_int),
+        "fdk_adam_step": ([vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i64, vp], C.c_int),
+        "fdk_transmission_noise": ([vp, i64, C.c_double, C.c_double, C.c_uint64, vp], C.c_int),
+        "fdk_voxelize": ([G, vp, i32, vp, vp], C.c_int),
+        "fdk_rows_to_mirror": ([vp, vp, i64, i32, i32, vp], C.c_int),
+        "fdk_volume_mse": ([vp, vp, vp, i32, i32, i32, f64p, vp], C.c_int),
+        "fdk_bp_adjoint": ([G, vp, vp, i32, vp, vp], C.c_int),
         "fdk_probe_smem": ([i32, f64p], C.c_int),
         "fdk_probe_fma": ([i32, f64p], C.c_int),
     }

@@ -249,6 +249,46 @@ int fdk_recon_destroy(fdk_recon *h);
 int fdk_phantom_project(const fdk_geometry *g, const double *ell, int32_t n_ell, int64_t first,
                         int64_t n, float *dev_out, void *stream);
 
+/* ---- ray-marching forward projector: kernel_forwardProject
+ *      (genProj/cudaForwardProjection.cu:174-254, Text3DLinear genProj/cudaIterType.cuh:232-276) */
+/* dev_vol: device volume [z][y][x] (x fastest) of g's size.  Writes views first..first+n-1, nv x nu
+ * each, to dev_out: per detector pixel, trilinear samples every min(dx, dy, dz) mm along the ray
+ * inside the voxel-centre box, times the step.  Asynchronous on stream (returns after queueing). */
+int fdk_forward_project(const fdk_geometry *g, const float *dev_vol, int64_t first, int64_t n, float *dev_out,
+                        void *stream);
+
+/* ---- learned residual row filter and its training kernels (no reference counterpart) -------
+ * Network per detector row x (length <= 256): a1 = relu(W1*(s x)+b1) (1->32 channels, kernel 9,
+ * zero 'same' padding), a2 = relu(W2*a1+b2) (32->32), o = W3*a2+b3 (32->1), y = x + o/s; s scales
+ * rows to line-integral units.  Parameters FP32 in the order W1[32][9], b1[32], W2[32][32][9], b2[32],
+ * W3[32][9], b3 (fdk_nn_param_count() floats); activations BF16 in shared memory. */
+int fdk_nn_param_count(void);
+/* y = x + net(x) for `rows` rows of `len` samples (device, row-major). */
+int fdk_nn_forward(const float *params, const float *x, float *y, int64_t rows, int32_t len, float scale,
+                   void *stream);
+/* Parameter gradient dparams (overwritten) of sum(dy . y) over all rows; recomputes activations. */
+int fdk_nn_backward(const float *params, const float *x, const float *dy, float *dparams, int64_t rows,
+                    int32_t len, float scale, void *stream);
+/* One Adam step (bias-corrected, step t >= 1) on n parameters. */
+int fdk_adam_step(float *params, const float *grads, float *m, float *v, int64_t n, float lr, float beta1,
+                  float beta2, float eps, int64_t t, void *stream);
+/* Low-dose transmission data in place: p -> -log(max(Poisson(I0 exp(-mu p)), 1) / I0) / mu. */
+int fdk_transmission_noise(float *dev_views, int64_t n, double i0, double mu, uint64_t seed, void *stream);
+/* Ellipsoid phantom (records as fdk_phantom_project) sampled at voxel centres, [z][y][x]. */
+int fdk_voxelize(const fdk_geometry *g, const double *ell, int32_t n_ell, float *dev_vol, void *stream);
+/* ROWS views (n x nv x nu) -> MIRROR f32 pairs (n x nu x nv x 2), the staged backprojection's input. */
+int fdk_rows_to_mirror(const float *dev_rows, void *dev_mirror, int64_t n_views, int32_t nu, int32_t nv,
+                       void *stream);
+/* Sum of squared errors of a backprojection volume ([x][y][z], as fdk_bp_volume_device of a full slab
+ * pair) against truth ([z][y][x]) into *sse_host; dev_res (may be NULL) = 2 (vol - truth) / N, [z][y][x]. */
+int fdk_volume_mse(const float *dev_vol_xyz, const float *dev_truth, float *dev_res, int32_t nx, int32_t ny,
+                   int32_t nz, double *sse_host, void *stream);
+/* Exact adjoint of the staged backprojection (FDK_BP_FP32 semantics) over the whole slab pair:
+ * dev_grad (ROWS, n_views x nv x nu, accumulated) += BP^T(dev_res [z][y][x]).  dev_mats: device, 12
+ * per view. */
+int fdk_bp_adjoint(const fdk_geometry *g, const float *dev_res, const float *dev_mats, int32_t n_views,
+                   float *dev_grad, void *stream);
+
 /* ---- measurement probes (no reference counterpart) ------------------------ */
 /* The backprojection is bound by shared-memory bandwidth or FP32 issue rate; these measure the
  * two denominators of its roofline on the given device: conflict-free 128-bit shared-memory

@@ -502,3 +502,69 @@ void orc_ellipsoid_volume(const double *ell, int n_ell, long nx, long ny, long n
                 out[(z * ny + y) * nx + x] = (float)v;
             }
 }
+
+/* ------------------------------------------------------------------------- */
+/* ray-marching forward projector                                            */
+/* ------------------------------------------------------------------------- */
+
+static inline float vox_clamp(const float *vol, long nx, long ny, long nz, long x, long y, long z)
+{
+    x = x < 0 ? 0 : (x >= nx ? nx - 1 : x);
+    y = y < 0 ? 0 : (y >= ny ? ny - 1 : y);
+    z = z < 0 ? 0 : (z >= nz ? nz - 1 : z);
+    return vol[(z * ny + y) * nx + x];
+}
+
+/* kernel_forwardProject (genProj/cudaForwardProjection.cu:174-254) for one view, FP32 as the
+ * reference: the projector rotates by -angle (:426), cuRotate (x c - y s, x s + y c); ray from the
+ * source (0, -SOD, 0) to the pixel (u_mm, SID-SOD, v_mm), normalised (:216); cuIntersectBox with the
+ * voxel-centre box (:28-48, cudaIterType.cuh:189-199); samples every min(dx,dy,dz) from t_near while
+ * t < t_far (:240); Text3DLinear: int3 truncation, texels clamped to the volume, blend z, then y,
+ * then x (cudaIterType.cuh:256-270); value = sum * step (:249).  vol [z][y][x]; out nv x nu. */
+void orc_forward_project(const float *vol, long nx, long ny, long nz, float dx, float dy, float dz, long nu,
+                         long nv, float du, float dv, float sid, float sod, double angle_bp, float *out)
+{
+    const double ang = -angle_bp;
+    const float c = (float)cos(ang), s = (float)sin(ang);
+    const float src_y = -sod, det_y = sid - sod;
+    const float ox = -src_y * s, oy = src_y * c, oz = 0.f;
+    const float cu = (nu - 1) / 2.0f, cv = (nv - 1) / 2.0f;
+    const float bx = (nx - 1) / 2.0f * dx, by = (ny - 1) / 2.0f * dy, bz = (nz - 1) / 2.0f * dz;
+    const float step = fminf(fminf(dx, dy), dz);
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < nv; j++)
+        for (long i = 0; i < nu; i++) {
+            const float umm = ((float)i - cu) * du, vmm = (cv - (float)j) * dv;
+            const float px = umm * c - det_y * s, py = umm * s + det_y * c, pz = vmm;
+            float dxr = px - ox, dyr = py - oy, dzr = pz - oz;
+            const float inv = 1.0f / sqrtf(dxr * dxr + dyr * dyr + dzr * dzr);
+            dxr *= inv;
+            dyr *= inv;
+            dzr *= inv;
+            const float tx0 = (-bx - ox) / dxr, tx1 = (bx - ox) / dxr;
+            const float ty0 = (-by - oy) / dyr, ty1 = (by - oy) / dyr;
+            const float tz0 = (-bz - oz) / dzr, tz1 = (bz - oz) / dzr;
+            const float tnear = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fminf(tz0, tz1));
+            const float tfar = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+            float sum = 0.f;
+            if (tfar > tnear) {
+                const float si = ox / dx + (nx - 1) / 2.0f, sj = (ny - 1) / 2.0f - oy / dy,
+                            sk = (nz - 1) / 2.0f - oz / dz;
+                const float vi = dxr / dx, vj = -dyr / dy, vk = -dzr / dz;
+                for (float t = tnear; t < tfar; t += step) {
+                    const float pi = si + vi * t, pj = sj + vj * t, pk = sk + vk * t;
+                    const long ai = (long)pi, aj = (long)pj, ak = (long)pk;
+                    const float fi = pi - ai, fj = pj - aj, fk = pk - ak;
+#define V(a, b, cc) vox_clamp(vol, nx, ny, nz, a, b, cc)
+                    const float c00 = V(ai, aj, ak) * (1 - fk) + V(ai, aj, ak + 1) * fk;
+                    const float c10 = V(ai + 1, aj, ak) * (1 - fk) + V(ai + 1, aj, ak + 1) * fk;
+                    const float c01 = V(ai, aj + 1, ak) * (1 - fk) + V(ai, aj + 1, ak + 1) * fk;
+                    const float c11 = V(ai + 1, aj + 1, ak) * (1 - fk) + V(ai + 1, aj + 1, ak + 1) * fk;
+#undef V
+                    const float f0 = c00 * (1 - fj) + c01 * fj, f1 = c10 * (1 - fj) + c11 * fj;
+                    sum += f0 * (1 - fi) + f1 * fi;
+                }
+            }
+            out[j * nu + i] = sum * step;
+        }
+}

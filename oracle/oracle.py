@@ -65,6 +65,8 @@ def lib():
                                                C.c_double, C.c_double, C.c_double, C.c_double, _f32p]
         L.orc_ellipsoid_volume.argtypes = [_f64p, C.c_int, C.c_long, C.c_long, C.c_long,
                                            C.c_double, C.c_double, C.c_double, _f32p]
+        L.orc_forward_project.argtypes = ([_f32p] + [C.c_long] * 3 + [C.c_float] * 3 + [C.c_long] * 2 +
+                                          [C.c_float] * 4 + [C.c_double, _f32p])
         _lib = L
     return _lib
 
@@ -173,6 +175,14 @@ def ellipsoid_volume(ell: np.ndarray, g) -> np.ndarray:
     out = np.zeros((g.nz, g.ny, g.nx), np.float32)
     e = np.ascontiguousarray(ell, np.float64).reshape(-1)
     lib().orc_ellipsoid_volume(e, len(e) // 16, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, out)
+    return out
+
+
+def forward_project(vol: np.ndarray, g, angle: float) -> np.ndarray:
+    """Ray-marching projector (genProj kernel_forwardProject semantics) of a [z][y][x] volume."""
+    out = np.zeros((g.nv, g.nu), np.float32)
+    lib().orc_forward_project(np.ascontiguousarray(vol, np.float32).reshape(-1), g.nx, g.ny, g.nz, g.dx, g.dy,
+                              g.dz, g.nu, g.nv, g.du, g.dv, g.SID, g.SOD, float(angle), out)
     return out
 
 
