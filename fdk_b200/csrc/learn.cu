@@ -19,6 +19,7 @@
 // ROWS -> MIRROR layout change that feeds the backprojection.
 #include <cuda_bf16.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.h"
@@ -29,182 +30,389 @@ namespace fdk {
 constexpr int kCh = 32, kK = 9, kHalo = 4;
 constexpr int kW1 = 0, kB1 = kW1 + kCh * kK, kW2 = kB1 + kCh, kB2 = kW2 + kCh * kCh * kK, kW3 = kB2 + kCh,
               kB3 = kW3 + kCh * kK, kNParam = kB3 + 1;
-constexpr int kMaxLen = 256;  // row length limit (threads per CTA = row length; smem ~180 KB backward)
+constexpr int kMaxLen = 256;  // row length limit (the backward kernel holds ~176 KB of shared memory)
 
 // --------------------------------------------------------------------------------------------
-// fused forward (inference): one CTA per row, thread = position
+// Network kernels.  One CTA of 256 threads works on one row at a time (persistent over rows).
+// The convolutions are register-blocked: in the channel phases thread t owns 4 consecutive
+// positions (pg = t % 64) x 8 channels (q = t / 64, uniform within a warp), so each float4
+// weight load (a warp-wide broadcast) feeds 16 FMAs and one 12-value activation window feeds
+// all 9 taps.  Activation rows carry a zero halo: buffer index = position + 4, and every entry
+// past the row's end stays zero, so no tap needs a bounds test.
 // --------------------------------------------------------------------------------------------
-struct NnShared {
-    float w[kNParam];                            // all parameters
-    __nv_bfloat16 a1[kCh][kMaxLen + 2 * kHalo];  // layer-1 activations, zero halo
-    float x[kMaxLen + 2 * kHalo];
+constexpr int kThreads = 256;
+constexpr int kBuf = kMaxLen + 2 * kHalo + 8;  // 272 f32 per scalar row buffer (x, d3)
+constexpr int kPitchA = 268;                    // bf16 per activation row (8-byte aligned rows)
+constexpr int kPitchD = 268;                    // f32 per dz2 row (16-byte aligned rows)
+constexpr int kPitchZ = 260;                    // f32 per dz1 row (16-byte aligned rows)
+
+struct NnWeights {
+    float w2f[kCh * kK * kCh];  // W2 as [ci][k][c]: the 8 output channels of one (ci, k) are contiguous
+    float w1[kCh * kK], b1[kCh], b2[kCh], w3[kCh * kK], b3[4];
 };
 
-__device__ __forceinline__ void nn_load(NnShared &sm, const float *params, const float *xrow, int L, float s) {
-    for (int i = threadIdx.x; i < kNParam; i += blockDim.x) sm.w[i] = params[i];
-    for (int i = threadIdx.x; i < L + 2 * kHalo; i += blockDim.x) {
-        const int p = i - kHalo;
-        sm.x[i] = (p >= 0 && p < L) ? xrow[p] * s : 0.f;
-        if (i < kHalo || i >= L + kHalo)
-            for (int c = 0; c < kCh; c++) sm.a1[c][i] = __float2bfloat16(0.f);
+struct NnFwdShared {
+    NnWeights w;
+    float x[kBuf];                        // s * x with halo
+    float part[4][kMaxLen];               // layer-3 partial sums of the 4 channel groups
+    __nv_bfloat16 a1[kCh][kPitchA];       // relu(layer 1), BF16
+    __nv_bfloat16 a2[kCh][kPitchA];       // relu(layer 2), BF16
+};
+
+__device__ __forceinline__ float bf_lo(unsigned u) { return __uint_as_float(u << 16); }
+__device__ __forceinline__ float bf_hi(unsigned u) { return __uint_as_float(u & 0xFFFF0000u); }
+
+// 12 consecutive f32 from a 16-byte aligned address
+__device__ __forceinline__ void ld_f12(const float *p, float (&v)[12]) {
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const float4 t = reinterpret_cast<const float4 *>(p)[i];
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
     }
 }
 
-// a1 for this thread's position (pre-activation returned in z1 when requested)
-__device__ __forceinline__ void nn_layer1(NnShared &sm, int p, int L) {
-    if (p >= L) return;
-#pragma unroll 4
-    for (int c = 0; c < kCh; c++) {
-        float z = sm.w[kB1 + c];
+// 4n consecutive BF16 (as f32) from an 8-byte aligned address
+template <int N>
+__device__ __forceinline__ void ld_bf(const __nv_bfloat16 *p, float (&v)[N]) {
+    static_assert(N % 4 == 0, "groups of 4");
 #pragma unroll
-        for (int k = 0; k < kK; k++) z = fmaf(sm.w[kW1 + c * kK + k], sm.x[p + k], z);
-        sm.a1[c][p + kHalo] = __float2bfloat16(fmaxf(z, 0.f));
+    for (int i = 0; i < N / 4; i++) {
+        const uint2 u = reinterpret_cast<const uint2 *>(p)[i];
+        v[4 * i] = bf_lo(u.x);
+        v[4 * i + 1] = bf_hi(u.x);
+        v[4 * i + 2] = bf_lo(u.y);
+        v[4 * i + 3] = bf_hi(u.y);
     }
 }
 
-// z2[c] for all 32 output channels of this position
-__device__ __forceinline__ void nn_layer2(const NnShared &sm, int p, float (&z2)[kCh]) {
+// 4 values -> BF16 (round to nearest even) at an 8-byte aligned address
+__device__ __forceinline__ void st_bf4(__nv_bfloat16 *p, const float (&v)[4]) {
+    const __nv_bfloat162 lo = __floats2bfloat162_rn(v[0], v[1]), hi = __floats2bfloat162_rn(v[2], v[3]);
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned *>(&lo);
+    u.y = *reinterpret_cast<const unsigned *>(&hi);
+    *reinterpret_cast<uint2 *>(p) = u;
+}
+
+__device__ void nn_load_weights(NnWeights &w, float *w2b, const float *params) {
+    for (int i = threadIdx.x; i < kCh * kCh * kK; i += kThreads) {
+        const int c = i / (kCh * kK), ci = (i / kK) % kCh, k = i % kK;  // params W2[c][ci][k]
+        const float v = params[kW2 + i];
+        w.w2f[(ci * kK + k) * kCh + c] = v;
+        if (w2b) w2b[(c * kK + k) * kCh + ci] = v;
+    }
+    for (int i = threadIdx.x; i < kCh * kK; i += kThreads) {
+        w.w1[i] = params[kW1 + i];
+        w.w3[i] = params[kW3 + i];
+    }
+    for (int i = threadIdx.x; i < kCh; i += kThreads) {
+        w.b1[i] = params[kB1 + i];
+        w.b2[i] = params[kB2 + i];
+    }
+    if (threadIdx.x == 0) w.b3[0] = params[kB3];
+}
+
+// a1[c][p] = relu(b1[c] + sum_k W1[c][k] xs[p + k - 4]) for this thread's 4 positions x 8 channels
+__device__ __forceinline__ void nn_layer1(const NnWeights &w, const float *xb, __nv_bfloat16 (*a1)[kPitchA], int pg,
+                                          int q, int L) {
+    const int p0 = 4 * pg;
+    float xw[12];
+    ld_f12(xb + p0, xw);  // positions p0 - 4 .. p0 + 7
 #pragma unroll
-    for (int c = 0; c < kCh; c++) z2[c] = sm.w[kB2 + c];
-    for (int ci = 0; ci < kCh; ci++) {
+    for (int i = 0; i < 8; i++) {
+        const int c = 8 * q + i;
+        float z[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) z[j] = w.b1[c];
 #pragma unroll
         for (int k = 0; k < kK; k++) {
-            const float a = __bfloat162float(sm.a1[ci][p + k]);
+            const float wk = w.w1[c * kK + k];
 #pragma unroll
-            for (int c = 0; c < kCh; c++) z2[c] = fmaf(sm.w[kW2 + (c * kCh + ci) * kK + k], a, z2[c]);
+            for (int j = 0; j < 4; j++) z[j] = fmaf(wk, xw[j + k], z[j]);
         }
+#pragma unroll
+        for (int j = 0; j < 4; j++) z[j] = (p0 + j < L) ? fmaxf(z[j], 0.f) : 0.f;
+        st_bf4(&a1[c][p0 + kHalo], z);
     }
 }
 
-__global__ void __launch_bounds__(kMaxLen) nn_forward_kernel(const float *__restrict__ params, const float *x, float *y,
-                                                            int L, long long rows, float s) {
+// a2[c][p] = relu(b2[c] + sum_ci sum_k W2[c][ci][k] a1[ci][p + k - 4])
+__device__ __forceinline__ void nn_layer2(const NnWeights &w, const __nv_bfloat16 (*a1)[kPitchA],
+                                          __nv_bfloat16 (*a2)[kPitchA], int pg, int q, int L) {
+    const int p0 = 4 * pg;
+    float acc[8][4];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = w.b2[8 * q + i];
+#pragma unroll 2
+    for (int ci = 0; ci < kCh; ci++) {
+        float a[12];
+        ld_bf<12>(&a1[ci][p0], a);
+#pragma unroll
+        for (int k = 0; k < kK; k++) {
+            const float4 wa = *reinterpret_cast<const float4 *>(&w.w2f[(ci * kK + k) * kCh + 8 * q]);
+            const float4 wb = *reinterpret_cast<const float4 *>(&w.w2f[(ci * kK + k) * kCh + 8 * q + 4]);
+            const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = fmaf(wv[i], a[j + k], acc[i][j]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        float r[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) r[j] = (p0 + j < L) ? fmaxf(acc[i][j], 0.f) : 0.f;
+        st_bf4(&a2[8 * q + i][p0 + kHalo], r);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 2) nn_forward_kernel(const float *__restrict__ params, const float *x,
+                                                                float *y, int L, long long rows, float s) {
     extern __shared__ __align__(16) unsigned char smraw[];
-    NnShared &sm = *reinterpret_cast<NnShared *>(smraw);
-    __shared__ __nv_bfloat16 a2s[kCh][kMaxLen + 2 * kHalo];
-    const int p = threadIdx.x;
+    NnFwdShared &sm = *reinterpret_cast<NnFwdShared *>(smraw);
+    const int t = threadIdx.x, pg = t % 64, q = t / 64;
+    nn_load_weights(sm.w, nullptr, params);
+    for (int i = t; i < kCh * kPitchA; i += kThreads) {
+        (&sm.a1[0][0])[i] = __float2bfloat16(0.f);
+        (&sm.a2[0][0])[i] = __float2bfloat16(0.f);
+    }
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         __syncthreads();
-        nn_load(sm, params, x + r * L, L, s);
-        if (p < kCh)
-            for (int i = 0; i < kHalo; i++) {
-                a2s[p][i] = __float2bfloat16(0.f);
-                a2s[p][L + kHalo + i] = __float2bfloat16(0.f);
-            }
-        __syncthreads();
-        nn_layer1(sm, p, L);
-        __syncthreads();
-        if (p < L) {
-            float z2[kCh];
-            nn_layer2(sm, p, z2);
-#pragma unroll
-            for (int c = 0; c < kCh; c++) a2s[c][p + kHalo] = __float2bfloat16(fmaxf(z2[c], 0.f));
+        for (int i = t; i < kBuf; i += kThreads) {
+            const int p = i - kHalo;
+            sm.x[i] = (p >= 0 && p < L) ? x[r * L + p] * s : 0.f;
         }
         __syncthreads();
-        if (p < L) {
-            float o = sm.w[kB3];
-            for (int c = 0; c < kCh; c++)
+        nn_layer1(sm.w, sm.x, sm.a1, pg, q, L);
+        __syncthreads();
+        nn_layer2(sm.w, sm.a1, sm.a2, pg, q, L);
+        __syncthreads();
+        {  // layer 3, partial over this thread's 8 channels
+            float o[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-                for (int k = 0; k < kK; k++) o = fmaf(sm.w[kW3 + c * kK + k], __bfloat162float(a2s[c][p + k]), o);
-            y[r * L + p] = x[r * L + p] + o / s;
+            for (int i = 0; i < 8; i++) {
+                const int c = 8 * q + i;
+                float a[12];
+                ld_bf<12>(&sm.a2[c][4 * pg], a);
+#pragma unroll
+                for (int k = 0; k < kK; k++) {
+                    const float wk = sm.w.w3[c * kK + k];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) o[j] = fmaf(wk, a[j + k], o[j]);
+                }
+            }
+            *reinterpret_cast<float4 *>(&sm.part[q][4 * pg]) = make_float4(o[0], o[1], o[2], o[3]);
+        }
+        __syncthreads();
+        if (t < L) {
+            const float o = sm.w.b3[0] + ((sm.part[0][t] + sm.part[1][t]) + (sm.part[2][t] + sm.part[3][t]));
+            y[r * L + t] = x[r * L + t] + o / s;
         }
     }
 }
 
 // --------------------------------------------------------------------------------------------
-// backward: persistent CTAs, rows recomputed, parameter gradients accumulated per CTA
+// backward: persistent CTAs (one per SM); each row's activations are recomputed in shared
+// memory, and the parameter gradients stay in registers for the CTA's whole life:
+//   dW2[c][ci][k]  thread (warp w: c = 4w..4w+3, lane: ci), 36 accumulators
+//   dW3[c][k], dW1[ci][k]  lane = channel, warp = a 32-position range, 9 accumulators each
+//   db1, db2 (8 per thread, its channel group), db3
+// and are added to global memory once at the end.
 // --------------------------------------------------------------------------------------------
 struct NnBackShared {
-    NnShared f;
-    __nv_bfloat16 a2[kCh][kMaxLen + 2 * kHalo];
-    float dz2[kCh][kMaxLen + 2 * kHalo];  // gradient of layer-2 pre-activation, zero halo
-    float dz1[kCh][kMaxLen];               // gradient of layer-1 pre-activation
-    float d3[kMaxLen + 2 * kHalo];         // dL/do (output gradient, scaled), zero halo
-    float gw[kNParam];                     // this CTA's parameter gradients
+    NnWeights w;
+    float w2b[kCh * kK * kCh];        // W2 as [c][k][ci]: the 8 input channels of one (c, k) are contiguous
+    float x[kBuf];                    // s * x with halo
+    float d3[kBuf];                   // dL/do = dL/dy / s with halo
+    float dz2[kCh][kPitchD];          // dL/dz2 with halo
+    float dz1[kCh][kPitchZ];          // dL/dz1, positions 0 .. 255
+    __nv_bfloat16 a1[kCh][kPitchA];
+    __nv_bfloat16 a2[kCh][kPitchA];
 };
 
-__global__ void __launch_bounds__(kMaxLen) nn_backward_kernel(const float *__restrict__ params, const float *x,
-                                                             const float *dy, float *dparams, int L, long long rows,
-                                                             float s) {
+__global__ void __launch_bounds__(kThreads, 1) nn_backward_kernel(const float *__restrict__ params, const float *x,
+                                                                 const float *dy, float *dparams, int L,
+                                                                 long long rows, float s) {
     extern __shared__ __align__(16) unsigned char smraw[];
     NnBackShared &sm = *reinterpret_cast<NnBackShared *>(smraw);
-    const int p = threadIdx.x;
-    for (int i = p; i < kNParam; i += blockDim.x) sm.gw[i] = 0.f;
+    const int t = threadIdx.x, pg = t % 64, q = t / 64, p0 = 4 * pg, lane = t & 31, wp = t >> 5;
+    nn_load_weights(sm.w, sm.w2b, params);
+    for (int i = t; i < kCh * kPitchA; i += kThreads) {
+        (&sm.a1[0][0])[i] = __float2bfloat16(0.f);
+        (&sm.a2[0][0])[i] = __float2bfloat16(0.f);
+    }
+    for (int i = t; i < kCh * kPitchD; i += kThreads) (&sm.dz2[0][0])[i] = 0.f;
+
+    float gw2[4][kK], gw3[kK], gw1[kK], gb1[8], gb2[8], gb3 = 0.f;
+#pragma unroll
+    for (int k = 0; k < kK; k++) {
+        gw3[k] = gw1[k] = 0.f;
+#pragma unroll
+        for (int i = 0; i < 4; i++) gw2[i][k] = 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) gb1[i] = gb2[i] = 0.f;
+
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         __syncthreads();
-        nn_load(sm.f, params, x + r * L, L, s);
-        for (int i = p; i < L + 2 * kHalo; i += blockDim.x) {
-            const int q = i - kHalo;
-            // y = x + o / s  ->  dL/do = dL/dy / s
-            sm.d3[i] = (q >= 0 && q < L) ? dy[r * L + q] / s : 0.f;
-            if (i < kHalo || i >= L + kHalo)
-                for (int c = 0; c < kCh; c++) {
-                    sm.a2[c][i] = __float2bfloat16(0.f);
-                    sm.dz2[c][i] = 0.f;
+        for (int i = t; i < kBuf; i += kThreads) {
+            const int p = i - kHalo;
+            const bool in = p >= 0 && p < L;
+            sm.x[i] = in ? x[r * L + p] * s : 0.f;
+            const float d = in ? dy[r * L + p] / s : 0.f;  // y = x + o / s
+            sm.d3[i] = d;
+            gb3 += d;
+        }
+        __syncthreads();
+        nn_layer1(sm.w, sm.x, sm.a1, pg, q, L);
+        __syncthreads();
+        nn_layer2(sm.w, sm.a1, sm.a2, pg, q, L);
+        __syncthreads();
+        {  // dz2[c][p] = [a2 > 0] sum_k W3[c][k] d3[p - k + 4]
+            float dw[12];
+            ld_f12(sm.d3 + p0, dw);  // positions p0 - 4 .. p0 + 7
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+                const int c = 8 * q + i;
+                float m[4];
+                ld_bf<4>(&sm.a2[c][p0 + kHalo], m);
+                float g[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int k = 0; k < kK; k++) {
+                    const float wk = sm.w.w3[c * kK + k];
+#pragma unroll
+                    for (int j = 0; j < 4; j++) g[j] = fmaf(wk, dw[j - k + 8], g[j]);
                 }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    g[j] = m[j] > 0.f ? g[j] : 0.f;
+                    gb2[i] += g[j];
+                }
+                *reinterpret_cast<float4 *>(&sm.dz2[c][p0 + kHalo]) = make_float4(g[0], g[1], g[2], g[3]);
+            }
+        }
+        // dW3[c][k] += sum_p d3[p] a2[c][p + k - 4]   (lane = c, warp = positions 32 wp ..)
+#pragma unroll 1
+        for (int m = 0; m < 4; m++) {
+            const int pb = 32 * wp + 8 * m;
+            if (pb >= L) break;
+            float a[16];
+            ld_bf<16>(&sm.a2[lane][pb], a);
+            const float4 d0 = *reinterpret_cast<const float4 *>(&sm.d3[pb + kHalo]);
+            const float4 d1 = *reinterpret_cast<const float4 *>(&sm.d3[pb + kHalo + 4]);
+            const float d[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+#pragma unroll
+                for (int k = 0; k < kK; k++) gw3[k] = fmaf(d[j], a[j + k], gw3[k]);
         }
         __syncthreads();
-        nn_layer1(sm.f, p, L);
-        __syncthreads();
-        float z2[kCh];
-        if (p < L) {
-            nn_layer2(sm.f, p, z2);
+        {  // dz1[ci][p] = [a1 > 0] sum_c sum_k W2[c][ci][k] dz2[c][p - k + 4]
+            float acc[8][4];
 #pragma unroll
-            for (int c = 0; c < kCh; c++) sm.a2[c][p + kHalo] = __float2bfloat16(fmaxf(z2[c], 0.f));
-        }
-        __syncthreads();
-        if (p < L) {
-            // dz2[c][p] = relu'(z2) * sum_k W3[c][k] d3[p - k + 4]   (transpose conv)
+            for (int i = 0; i < 8; i++)
 #pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+#pragma unroll 2
             for (int c = 0; c < kCh; c++) {
-                float g = 0.f;
+                float dw[12];
+                ld_f12(&sm.dz2[c][p0], dw);
 #pragma unroll
-                for (int k = 0; k < kK; k++) g = fmaf(sm.f.w[kW3 + c * kK + k], sm.d3[p + 2 * kHalo - k], g);
-                sm.dz2[c][p + kHalo] = z2[c] > 0.f ? g : 0.f;
-            }
-        }
-        __syncthreads();
-        if (p < L) {
-            // dz1[ci][p] = relu'(z1) * sum_c sum_k W2[c][ci][k] dz2[c][p - k + 4]
-            for (int ci = 0; ci < kCh; ci++) {
-                if (__bfloat162float(sm.f.a1[ci][p + kHalo]) <= 0.f) {
-                    sm.dz1[ci][p] = 0.f;
-                    continue;
+                for (int k = 0; k < kK; k++) {
+                    const float4 wa = *reinterpret_cast<const float4 *>(&sm.w2b[(c * kK + k) * kCh + 8 * q]);
+                    const float4 wb = *reinterpret_cast<const float4 *>(&sm.w2b[(c * kK + k) * kCh + 8 * q + 4]);
+                    const float wv[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(wv[i], dw[j - k + 8], acc[i][j]);
                 }
-                float g = 0.f;
-                for (int c = 0; c < kCh; c++)
+            }
 #pragma unroll
-                    for (int k = 0; k < kK; k++)
-                        g = fmaf(sm.f.w[kW2 + (c * kCh + ci) * kK + k], sm.dz2[c][p + 2 * kHalo - k], g);
-                sm.dz1[ci][p] = g;
+            for (int i = 0; i < 8; i++) {
+                const int ci = 8 * q + i;
+                float m[4];
+                ld_bf<4>(&sm.a1[ci][p0 + kHalo], m);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    acc[i][j] = m[j] > 0.f ? acc[i][j] : 0.f;
+                    gb1[i] += acc[i][j];
+                }
+                *reinterpret_cast<float4 *>(&sm.dz1[ci][p0]) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+            }
+        }
+        // dW2[c][ci][k] += sum_p dz2[c][p] a1[ci][p + k - 4]   (c = 4 wp + i, lane = ci)
+#pragma unroll 1
+        for (int pb = 0; pb < L; pb += 8) {
+            float a[16];
+            ld_bf<16>(&sm.a1[lane][pb], a);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float4 d0 = *reinterpret_cast<const float4 *>(&sm.dz2[4 * wp + i][pb + kHalo]);
+                const float4 d1 = *reinterpret_cast<const float4 *>(&sm.dz2[4 * wp + i][pb + kHalo + 4]);
+                const float d[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+#pragma unroll
+                for (int j = 0; j < 8; j++)
+#pragma unroll
+                    for (int k = 0; k < kK; k++) gw2[i][k] = fmaf(d[j], a[j + k], gw2[i][k]);
             }
         }
         __syncthreads();
-        // parameter gradients of this row, summed over positions; thread t owns parameters t, t+B, ...
-        for (int i = p; i < kNParam; i += blockDim.x) {
-            float g = 0.f;
-            if (i < kB1) {  // W1[c][k]: sum_q dz1[c][q] * (s x)[q + k - 4]
-                const int c = i / kK, k = i % kK;
-                for (int q = 0; q < L; q++) g = fmaf(sm.dz1[c][q], sm.f.x[q + k], g);
-            } else if (i < kW2) {  // b1
-                const int c = i - kB1;
-                for (int q = 0; q < L; q++) g += sm.dz1[c][q];
-            } else if (i < kB2) {  // W2[c][ci][k]: sum_q dz2[c][q] * a1[ci][q + k - 4]
-                const int j = i - kW2, c = j / (kCh * kK), ci = (j / kK) % kCh, k = j % kK;
-                for (int q = 0; q < L; q++) g = fmaf(sm.dz2[c][q + kHalo], __bfloat162float(sm.f.a1[ci][q + k]), g);
-            } else if (i < kW3) {  // b2
-                const int c = i - kB2;
-                for (int q = 0; q < L; q++) g += sm.dz2[c][q + kHalo];
-            } else if (i < kB3) {  // W3[c][k]: sum_q d3[q] * a2[c][q + k - 4]
-                const int j = i - kW3, c = j / kK, k = j % kK;
-                for (int q = 0; q < L; q++) g = fmaf(sm.d3[q + kHalo], __bfloat162float(sm.a2[c][q + k]), g);
-            } else {  // b3
-                for (int q = 0; q < L; q++) g += sm.d3[q + kHalo];
+        // dW1[ci][k] += sum_p dz1[ci][p] xs[p + k - 4]   (lane = ci, warp = positions 32 wp ..)
+#pragma unroll 1
+        for (int m = 0; m < 4; m++) {
+            const int pb = 32 * wp + 8 * m;
+            if (pb >= L) break;
+            float xw[16];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const float4 v = *reinterpret_cast<const float4 *>(&sm.x[pb + 4 * i]);
+                xw[4 * i] = v.x;
+                xw[4 * i + 1] = v.y;
+                xw[4 * i + 2] = v.z;
+                xw[4 * i + 3] = v.w;
             }
-            sm.gw[i] += g;
+            const float4 g0 = *reinterpret_cast<const float4 *>(&sm.dz1[lane][pb]);
+            const float4 g1 = *reinterpret_cast<const float4 *>(&sm.dz1[lane][pb + 4]);
+            const float g[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+#pragma unroll
+                for (int k = 0; k < kK; k++) gw1[k] = fmaf(g[j], xw[j + k], gw1[k]);
         }
     }
-    __syncthreads();
-    for (int i = p; i < kNParam; i += blockDim.x) atomicAdd(dparams + i, sm.gw[i]);
+
+    // one global add per accumulator (db sums reduced over the warp's lanes first)
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int k = 0; k < kK; k++) atomicAdd(dparams + kW2 + ((4 * wp + i) * kCh + lane) * kK + k, gw2[i][k]);
+#pragma unroll
+    for (int k = 0; k < kK; k++) {
+        atomicAdd(dparams + kW3 + lane * kK + k, gw3[k]);
+        atomicAdd(dparams + kW1 + lane * kK + k, gw1[k]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+        for (int o = 16; o; o >>= 1) {
+            gb1[i] += __shfl_xor_sync(0xFFFFFFFFu, gb1[i], o);
+            gb2[i] += __shfl_xor_sync(0xFFFFFFFFu, gb2[i], o);
+        }
+    for (int o = 16; o; o >>= 1) gb3 += __shfl_xor_sync(0xFFFFFFFFu, gb3, o);
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            atomicAdd(dparams + kB1 + 8 * q + i, gb1[i]);
+            atomicAdd(dparams + kB2 + 8 * q + i, gb2[i]);
+        }
+        atomicAdd(dparams + kB3, gb3);
+    }
 }
 
 // --------------------------------------------------------------------------------------------
@@ -267,10 +475,14 @@ __global__ void noise_kernel(float *p, long long n, double i0, double mu, unsign
 // --------------------------------------------------------------------------------------------
 // ellipsoid voxelizer (value at voxel centres), [z][y][x]
 // --------------------------------------------------------------------------------------------
-__global__ void voxelize_kernel(const double *__restrict__ ell, int n_ell, int nx, int ny, int nz, double dx, double dy,
-                                double dz, float *out) {
+struct EllipsoidSet {  // passed by value: no device allocation or copy per call
+    double e[64 * 16];
+};
+
+__global__ void voxelize_kernel(const __grid_constant__ EllipsoidSet ell, int n_ell, int nx, int ny, int nz, double dx,
+                                double dy, double dz, float *out) {
     __shared__ double se[64 * 16];
-    for (int i = threadIdx.x; i < n_ell * 16; i += blockDim.x) se[i] = ell[i];
+    for (int i = threadIdx.x; i < n_ell * 16; i += blockDim.x) se[i] = ell.e[i];
     __syncthreads();
     const long long total = (long long)nx * ny * nz;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
@@ -321,6 +533,8 @@ __global__ void rows_to_mirror_kernel(const float *__restrict__ src, float2 *__r
 // volume MSE: vol in the backprojection's [x][y][z] layout, truth [z][y][x];
 // res[z][y][x] = 2 (vol - truth) / N, sum of squared errors in *sse
 // --------------------------------------------------------------------------------------------
+__device__ double g_sse;  // fdk_volume_mse's accumulator
+
 __global__ void mse_kernel(const float *__restrict__ vol, const float *__restrict__ truth, float *res, int nx, int ny,
                            int nz, double *sse) {
     const long long total = (long long)nx * ny * nz;
@@ -343,8 +557,21 @@ __global__ void mse_kernel(const float *__restrict__ vol, const float *__restric
 // 1/w^2 factor, SUBPIXEL's bounds -- into the view's ROWS-layout gradient.  One CTA: 16 x 16
 // columns x 8 top slices and their mirrors; per view, two shared-memory boxes (main rows and
 // mirror rows) collect the contributions before they are added to global memory.
+//
+// Contention: a warp covers 16 x 2 columns.  Per view the 16-wide side is laid along the
+// volume axis whose neighbours land on different detector columns (the larger |dU|), so the
+// lanes of one shared-memory atomic rarely hit the same address; both thread -> column
+// mappings keep their residuals in registers.  The boxes are double-buffered and zeroed by the
+// flush that reads them, so each view costs one barrier.
+//
+// Shared-memory float atomics run as load + compare-and-swap loops, so the boxes hold 32-bit
+// fixed point and take native integer atomics: per view every contribution w g is scaled by a
+// power of two S with |w g| S <= 2^19 for all voxels of the tile (the tile's largest |residual|
+// times the largest 1/w^2, found at its corners).  An entry sums at most one term per voxel, so
+// it stays below 2048 * 2^19 = 2^30; each term is rounded to the nearest 1/S.  The box is laid
+// out u-fastest, so the lanes of one atomic (consecutive detector columns) hit consecutive banks.
 // --------------------------------------------------------------------------------------------
-constexpr int kAdjR = 8, kAdjBH = 48, kAdjBW = 24;  // box: u rows x v columns
+constexpr int kAdjR = 8, kAdjBU = 48, kAdjBV = 24;  // box: u extent (fastest) x v extent
 
 struct AdjArgs {
     const float *res;   // [z][y][x]
@@ -353,52 +580,81 @@ struct AdjArgs {
     int n, nx, ny, nz, nu, nv;
 };
 
-__global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjArgs a) {
-    __shared__ float boxm[kAdjBH * kAdjBW], boxr[kAdjBH * kAdjBW];
-    __shared__ int meta[6];
+__global__ void __launch_bounds__(256, 3) bp_adjoint_kernel(AdjArgs a) {
+    __shared__ int box[2][2][kAdjBV * kAdjBU];  // [buffer][main, mirror], fixed point
+    __shared__ float warp_max[8];
     const int tid = threadIdx.x, lx = tid & 15, ly = tid >> 4;
-    const int xi = blockIdx.x * 16 + lx, yi = blockIdx.y * 16 + ly, zt = blockIdx.z * kAdjR;
-    const bool col_ok = xi < a.nx && yi < a.ny;
-    const int nzz = a.nz / 2;
-    float rm[kAdjR], rr[kAdjR];
+    const int zt = blockIdx.z * kAdjR, nzz = a.nz / 2;
+    // residuals of column (x0 + lx, y0 + ly) [mapping 0] and (x0 + ly, y0 + lx) [mapping 1]
+    float rm[2][kAdjR], rr[2][kAdjR];
+    bool col_ok[2];
 #pragma unroll
-    for (int k = 0; k < kAdjR; k++) {
-        const int z = zt + k;
-        const bool ok = col_ok && z < nzz;
-        rm[k] = ok ? a.res[((long long)z * a.ny + yi) * a.nx + xi] : 0.f;
-        rr[k] = ok ? a.res[((long long)(a.nz - 1 - z) * a.ny + yi) * a.nx + xi] : 0.f;
+    for (int mp = 0; mp < 2; mp++) {
+        const int xi = blockIdx.x * 16 + (mp ? ly : lx), yi = blockIdx.y * 16 + (mp ? lx : ly);
+        col_ok[mp] = xi < a.nx && yi < a.ny;
+#pragma unroll
+        for (int k = 0; k < kAdjR; k++) {
+            const int z = zt + k;
+            const bool ok = col_ok[mp] && z < nzz;
+            rm[mp][k] = ok ? a.res[((long long)z * a.ny + yi) * a.nx + xi] : 0.f;
+            rr[mp][k] = ok ? a.res[((long long)(a.nz - 1 - z) * a.ny + yi) * a.nx + xi] : 0.f;
+        }
     }
-    const float x = (float)xi, y = (float)yi, zf0 = (float)zt;
+    // largest |residual| of the tile: the fixed-point range
+    float gmax = 0.f;
+#pragma unroll
+    for (int k = 0; k < kAdjR; k++) gmax = fmaxf(gmax, fmaxf(fabsf(rm[0][k]), fabsf(rr[0][k])));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) gmax = fmaxf(gmax, __shfl_xor_sync(0xFFFFFFFFu, gmax, o));
+    if ((tid & 31) == 0) warp_max[tid >> 5] = gmax;
+    for (int i = tid; i < 2 * 2 * kAdjBV * kAdjBU; i += 256) (&box[0][0][0])[i] = 0;
+    __syncthreads();
+    gmax = warp_max[0];
+#pragma unroll
+    for (int i = 1; i < 8; i++) gmax = fmaxf(gmax, warp_max[i]);
+    if (!(gmax > 0.f)) return;  // the tile adds nothing (the whole CTA leaves together)
+    const float zf0 = (float)zt;
+    const int corner = tid & 3;
+    const float cx = blockIdx.x * 16 + ((corner & 1) ? 15 : 0), cy = blockIdx.y * 16 + ((corner & 2) ? 15 : 0);
     for (int s = 0; s < a.n; s++) {
         const float *m = a.mats + 12 * s;
-        if (tid == 0) {
-            // footprint of the block: corners of 16 x 16 columns x 8 slices (as the gather kernels)
-            float umin = 3e38f, umax = -3e38f, vmin = 3e38f, vmax = -3e38f;
-            for (int c = 0; c < 4; c++) {
-                const float cx = blockIdx.x * 16 + ((c & 1) ? 15 : 0), cy = blockIdx.y * 16 + ((c & 2) ? 15 : 0);
-                const float rw = 1.f / fmaf(m[8], cx, fmaf(m[9], cy, m[11]));
-                const float U = fmaf(m[0], cx, fmaf(m[1], cy, m[3])) * rw;
-                const float vw = fmaf(m[4], cx, fmaf(m[5], cy, m[7]));
-                const float va = fmaf(m[6], zf0, vw) * rw, vb = fmaf(m[6], zf0 + kAdjR - 1, vw) * rw;
-                umin = fminf(umin, U);
-                umax = fmaxf(umax, U);
-                vmin = fminf(vmin, fminf(va, vb));
-                vmax = fmaxf(vmax, fmaxf(va, vb));
+        const int cur = s & 1;
+        // footprint of the tile: lanes 4j .. 4j+3 evaluate one corner each (as the gather kernels)
+        float umin, umax, vmin, vmax, du_x, du_y, wtmax;
+        {
+            const float rw = 1.f / fmaf(m[8], cx, fmaf(m[9], cy, m[11]));
+            const float U = fmaf(m[0], cx, fmaf(m[1], cy, m[3])) * rw;
+            const float vw = fmaf(m[4], cx, fmaf(m[5], cy, m[7]));
+            const float va = fmaf(m[6], zf0, vw) * rw, vb = fmaf(m[6], zf0 + kAdjR - 1, vw) * rw;
+            umin = umax = U;
+            vmin = fminf(va, vb);
+            vmax = fmaxf(va, vb);
+            wtmax = rw * rw;  // 1/w is largest at a corner (w is linear in x, y)
+            const int base = tid & 28;  // lane of this group's corner 0
+            const float u0c = __shfl_sync(0xFFFFFFFFu, U, base);
+            du_x = __shfl_sync(0xFFFFFFFFu, U, base | 1) - u0c;
+            du_y = __shfl_sync(0xFFFFFFFFu, U, base | 2) - u0c;
+#pragma unroll
+            for (int o = 1; o <= 2; o <<= 1) {
+                umin = fminf(umin, __shfl_xor_sync(0xFFFFFFFFu, umin, o));
+                umax = fmaxf(umax, __shfl_xor_sync(0xFFFFFFFFu, umax, o));
+                vmin = fminf(vmin, __shfl_xor_sync(0xFFFFFFFFu, vmin, o));
+                vmax = fmaxf(vmax, __shfl_xor_sync(0xFFFFFFFFu, vmax, o));
+                wtmax = fmaxf(wtmax, __shfl_xor_sync(0xFFFFFFFFu, wtmax, o));
             }
-            const int u_lo = (int)floorf(umin) - 1, v_lo = (int)floorf(vmin) - 1;
-            const int rows = (int)floorf(umax) + 3 - u_lo, cols = (int)floorf(vmax) + 3 - v_lo;
-            meta[0] = u_lo;
-            meta[1] = v_lo;
-            meta[2] = rows;
-            meta[3] = cols;
-            meta[4] = (rows <= kAdjBH && cols <= kAdjBW) ? 1 : 0;
         }
-        for (int i = tid; i < kAdjBH * kAdjBW; i += 256) boxm[i] = boxr[i] = 0.f;
-        __syncthreads();
-        const int u_lo = meta[0], v_lo = meta[1], rows = meta[2], cols = meta[3];
-        const bool boxed = meta[4] != 0;
+        const int u_lo = (int)floorf(umin) - 1, v_lo = (int)floorf(vmin) - 1;
+        const int rows = (int)floorf(umax) + 3 - u_lo, cols = (int)floorf(vmax) + 3 - v_lo;  // u, v extents
+        const bool boxed = rows <= kAdjBU && cols <= kAdjBV;
+        const int mp = fabsf(du_y) > fabsf(du_x) ? 1 : 0;  // 16 lanes along the axis with the larger |dU|
+        int ex;
+        frexpf(gmax * wtmax * 1.0001f, &ex);  // |w g| <= gmax * wtmax < 2^ex
+        const int e = min(19 - ex, 126);
+        const float S = ldexpf(1.f, e), inv_s = ldexpf(1.f, -e);
+        int *boxm = box[cur][0], *boxr = box[cur][1];
         float *gv = a.grad + (long long)s * a.nu * a.nv;
-        if (col_ok) {
+        if (mp ? col_ok[1] : col_ok[0]) {
+            const float x = (float)(blockIdx.x * 16 + (mp ? ly : lx)), y = (float)(blockIdx.y * 16 + (mp ? lx : ly));
             const float rw = 1.f / fmaf(m[8], x, fmaf(m[9], y, m[11]));
             const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
             const float A = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], zf0, m[7]))) * rw;
@@ -420,15 +676,18 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjArgs a) {
                     const float fv = v - vf;
                     const float w00 = (1 - fu) * (1 - fv) * wt, w10 = fu * (1 - fv) * wt;
                     const float w01 = (1 - fu) * fv * wt, w11 = fu * fv * wt;
-                    if (mv && rm[k] != 0.f) {
+                    const float gm = mp ? rm[1][k] : rm[0][k];  // selects, not a dynamic register index
+                    const float gr = mp ? rr[1][k] : rr[0][k];
+                    if (mv && gm != 0.f) {
                         // main voxel: P[u0][vi], P[u0+1][vi], P[u0][vi+1], P[u0+1][vi+1]
-                        const float g = rm[k];
+                        const float g = gm;
                         if (boxed) {
-                            const int b = (u0 - u_lo) * kAdjBW + (vi - v_lo);
-                            atomicAdd(&boxm[b], w00 * g);
-                            atomicAdd(&boxm[b + kAdjBW], w10 * g);
-                            atomicAdd(&boxm[b + 1], w01 * g);
-                            atomicAdd(&boxm[b + kAdjBW + 1], w11 * g);
+                            const float gs = g * S;
+                            const int b = (vi - v_lo) * kAdjBU + (u0 - u_lo);
+                            atomicAdd(&boxm[b], __float2int_rn(w00 * gs));
+                            atomicAdd(&boxm[b + 1], __float2int_rn(w10 * gs));
+                            atomicAdd(&boxm[b + kAdjBU], __float2int_rn(w01 * gs));
+                            atomicAdd(&boxm[b + kAdjBU + 1], __float2int_rn(w11 * gs));
                         } else {
                             atomicAdd(&gv[(long long)vi * a.nu + u0], w00 * g);
                             atomicAdd(&gv[(long long)vi * a.nu + u0 + 1], w10 * g);
@@ -436,15 +695,16 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjArgs a) {
                             atomicAdd(&gv[(long long)(vi + 1) * a.nu + u0 + 1], w11 * g);
                         }
                     }
-                    if (rv && rr[k] != 0.f) {
+                    if (rv && gr != 0.f) {
                         // mirror voxel: weight (1-fv) on row nv-1-vi, fv on row nv-2-vi; box index by vi
-                        const float g = rr[k];
+                        const float g = gr;
                         if (boxed) {
-                            const int b = (u0 - u_lo) * kAdjBW + (vi - v_lo);
-                            atomicAdd(&boxr[b], w00 * g);
-                            atomicAdd(&boxr[b + kAdjBW], w10 * g);
-                            atomicAdd(&boxr[b + 1], w01 * g);
-                            atomicAdd(&boxr[b + kAdjBW + 1], w11 * g);
+                            const float gs = g * S;
+                            const int b = (vi - v_lo) * kAdjBU + (u0 - u_lo);
+                            atomicAdd(&boxr[b], __float2int_rn(w00 * gs));
+                            atomicAdd(&boxr[b + 1], __float2int_rn(w10 * gs));
+                            atomicAdd(&boxr[b + kAdjBU], __float2int_rn(w01 * gs));
+                            atomicAdd(&boxr[b + kAdjBU + 1], __float2int_rn(w11 * gs));
                         } else {
                             const long long r0 = a.nv - 1 - vi, r1 = a.nv - 2 - vi;
                             atomicAdd(&gv[r0 * a.nu + u0], w00 * g);
@@ -458,17 +718,20 @@ __global__ void __launch_bounds__(256) bp_adjoint_kernel(AdjArgs a) {
         }
         __syncthreads();
         if (boxed) {
-            // flush: box (u, c) with c = v - v_lo holds row v (main) / row nv-1-v (mirror), column u
+            // flush: entry (c, ru) = (v - v_lo, u - u_lo) holds row v (main) / row nv-1-v (mirror),
+            // column u; each entry is zeroed as it is read, ready for view s + 2
             for (int i = tid; i < rows * cols; i += 256) {
-                const int ru = i / cols, c = i - ru * cols;
+                const int c = i / rows, ru = i - c * rows;
+                const int bi = c * kAdjBU + ru;
+                const int qm = boxm[bi], qr = boxr[bi];
+                boxm[bi] = 0;
+                boxr[bi] = 0;
                 const int u = u_lo + ru, v = v_lo + c;
                 if (u < 0 || u >= a.nu || v < 0 || v >= a.nv) continue;
-                const float gm = boxm[ru * kAdjBW + c], gr = boxr[ru * kAdjBW + c];
-                if (gm != 0.f) atomicAdd(&gv[(long long)v * a.nu + u], gm);
-                if (gr != 0.f) atomicAdd(&gv[(long long)(a.nv - 1 - v) * a.nu + u], gr);
+                if (qm != 0) atomicAdd(&gv[(long long)v * a.nu + u], (float)qm * inv_s);
+                if (qr != 0) atomicAdd(&gv[(long long)(a.nv - 1 - v) * a.nu + u], (float)qr * inv_s);
             }
         }
-        __syncthreads();
     }
 }
 
@@ -485,10 +748,13 @@ int fdk_nn_forward(const float *params, const float *x, float *y, int64_t rows, 
     clear_error();
     FDK_CHECK_ARG(params && x && y, "NULL argument");
     FDK_CHECK_ARG(len >= kK && len <= kMaxLen && rows > 0, "row length must be 9..%d", kMaxLen);
-    const size_t smem = sizeof(NnShared);
+    const size_t smem = sizeof(NnFwdShared);
     FDK_CUDA(cudaFuncSetAttribute(nn_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int blocks = (int)std::min<long long>(rows, 148 * 8);
-    nn_forward_kernel<<<blocks, len, smem, (cudaStream_t)stream>>>(params, x, y, len, rows, scale);
+    int sms = 0, dev = 0;
+    FDK_CUDA(cudaGetDevice(&dev));
+    FDK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = (int)std::min<long long>(rows, 2 * sms);  // two resident CTAs per SM
+    nn_forward_kernel<<<blocks, kThreads, smem, (cudaStream_t)stream>>>(params, x, y, len, rows, scale);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
     FDK_ABI_END
@@ -507,7 +773,7 @@ int fdk_nn_backward(const float *params, const float *x, const float *dy, float 
     FDK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int blocks = (int)std::min<long long>(rows, sms);
     FDK_CUDA(cudaMemsetAsync(dparams, 0, sizeof(float) * kNParam, (cudaStream_t)stream));
-    nn_backward_kernel<<<blocks, len, smem, (cudaStream_t)stream>>>(params, x, dy, dparams, len, rows, scale);
+    nn_backward_kernel<<<blocks, kThreads, smem, (cudaStream_t)stream>>>(params, x, dy, dparams, len, rows, scale);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
     FDK_ABI_END
@@ -537,15 +803,11 @@ int fdk_transmission_noise(float *dev_views, int64_t n, double i0, double mu, ui
 int fdk_voxelize(const fdk_geometry *g, const double *ell, int32_t n_ell, float *dev_vol, void *stream) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(g && ell && dev_vol && n_ell >= 0 && n_ell <= 64, "bad arguments");
-    cudaStream_t st = (cudaStream_t)stream;
-    double *d_ell = nullptr;
-    FDK_CUDA(cudaMallocAsync((void **)&d_ell, sizeof(double) * 16 * (n_ell > 0 ? n_ell : 1), st));
-    if (n_ell > 0) FDK_CUDA(cudaMemcpyAsync(d_ell, ell, sizeof(double) * 16 * n_ell, cudaMemcpyHostToDevice, st));
-    voxelize_kernel<<<148 * 8, 256, 0, st>>>(d_ell, n_ell, (int)g->nx, (int)g->ny, (int)g->nz, g->dx, g->dy, g->dz,
-                                             dev_vol);
+    EllipsoidSet set;
+    for (int i = 0; i < 16 * n_ell; i++) set.e[i] = ell[i];
+    voxelize_kernel<<<148 * 8, 256, 0, (cudaStream_t)stream>>>(set, n_ell, (int)g->nx, (int)g->ny, (int)g->nz, g->dx,
+                                                               g->dy, g->dz, dev_vol);
     FDK_CUDA(cudaGetLastError());
-    FDK_CUDA(cudaFreeAsync(d_ell, st));
-    FDK_CUDA(cudaStreamSynchronize(st));
     return FDK_OK;
     FDK_ABI_END
 }
@@ -565,13 +827,15 @@ int fdk_volume_mse(const float *dev_vol_xyz, const float *dev_truth, float *dev_
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(dev_vol_xyz && dev_truth && sse_host && nx > 0 && ny > 0 && nz > 0, "bad arguments");
     cudaStream_t st = (cudaStream_t)stream;
+    // one accumulator per device (a module global), shared by the callers of that device in turn
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
     double *d_sse = nullptr;
-    FDK_CUDA(cudaMallocAsync((void **)&d_sse, sizeof(double), st));
+    FDK_CUDA(cudaGetSymbolAddress((void **)&d_sse, g_sse));
     FDK_CUDA(cudaMemsetAsync(d_sse, 0, sizeof(double), st));
     mse_kernel<<<148 * 8, 256, 0, st>>>(dev_vol_xyz, dev_truth, dev_res, nx, ny, nz, d_sse);
     FDK_CUDA(cudaGetLastError());
     FDK_CUDA(cudaMemcpyAsync(sse_host, d_sse, sizeof(double), cudaMemcpyDeviceToHost, st));
-    FDK_CUDA(cudaFreeAsync(d_sse, st));
     FDK_CUDA(cudaStreamSynchronize(st));
     return FDK_OK;
     FDK_ABI_END

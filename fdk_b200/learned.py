@@ -133,8 +133,9 @@ class Pipeline:
 
 
 def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 1000, params=None, log=print,
-          time_limit_s: float | None = None) -> dict:
-    """Adam on volume MSE, one phantom per step; the training scans are generated once."""
+          time_limit_s: float | None = None, on_epoch=None) -> dict:
+    """Adam on volume MSE, one phantom per step; the training scans are generated once.
+    on_epoch(epoch, params, history), when given, runs after every epoch (checkpointing)."""
     import torch
 
     pl = Pipeline()
@@ -169,10 +170,12 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
         n_done = len(order) if not stopped else (step - ep * n_train)
         hist.append(tot / max(1, n_done))
         log(f"epoch {ep}: train MSE {hist[-1]:.4e} ({time.time() - t0:.0f} s, {step} steps)")
+        if on_epoch is not None:
+            on_epoch(ep, w.cpu().numpy(), list(hist))
         if stopped:
             break
     return {"params": w.cpu().numpy(), "history": hist, "steps": step, "seconds": time.time() - t0,
-            "epochs_completed": len(hist) if not stopped else len(hist) - 1 + 0, "stopped_early": stopped}
+            "epochs_completed": len(hist) if not stopped else len(hist) - 1, "stopped_early": stopped}
 
 
 def evaluate(params, n_test: int = 200, seed0: int = 5000) -> dict:

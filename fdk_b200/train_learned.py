@@ -34,8 +34,12 @@ def main():
     args = ap.parse_args()
     log = lambda *a: print(*a, file=sys.stderr, flush=True)  # noqa: E731
     t0 = time.time()
-    tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit)
-    os.makedirs(os.path.dirname(args.out), exist_ok=True)
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+
+    def checkpoint(ep, params, hist):
+        np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * args.n_train)
+
+    tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit, on_epoch=checkpoint)
     np.savez(args.out, params=tr["params"], history=np.asarray(tr["history"]), steps=tr["steps"])
     ev = learned.evaluate(tr["params"], args.n_test)
     out = {"workload": "C5: 256^3, 90 views of 256^2, I0=1e4, mu=0.02/mm", "n_train": args.n_train,

@@ -82,6 +82,42 @@ def test_network_kernels_vs_cpu_oracle():
     assert Lr.n_params() == N.NPARAM
 
 
+def test_end_to_end_gradient_finite_difference():
+    """Directional derivative of the volume MSE along the last layer (W3, b3), where the loss is
+    exactly quadratic in the step, from the gradient kernels (backprojection adjoint + network
+    backward) against a central difference through the forward pipeline (network + BP + MSE)."""
+    import torch
+
+    p = small_param(40, 40, 40, 24)
+    pl = Lr.Pipeline(p)
+    x = torch.empty((p.nProj, p.nv, p.nu), dtype=torch.float32, device="cuda")
+    pl.scan(7, x)
+    rng = np.random.default_rng(3)
+    w0 = Lr.init_params()
+    k_w3 = N.NPARAM - 32 * 9 - 1
+    w0[k_w3:] = (rng.standard_normal(32 * 9 + 1) * 0.05).astype(np.float32)
+    d = np.zeros_like(w0)
+    d[k_w3:] = rng.standard_normal(32 * 9 + 1).astype(np.float32)
+
+    def loss(w_host, grad=False):
+        w = torch.from_numpy(w_host).cuda()
+        pl.truth_of(7)
+        pl.reconstruct(w, x)
+        e = pl.mse(grad)
+        if grad:
+            pl.gradient(w, x)
+            torch.cuda.synchronize()
+            return e, pl.dparams.cpu().numpy().astype(np.float64)
+        return e
+
+    l0, g = loss(w0, grad=True)
+    t = 0.05 * l0 / abs(float(g @ d))
+    wp, wm = (w0 + t * d).astype(np.float32), (w0 - t * d).astype(np.float32)
+    predicted = float(g @ (wp.astype(np.float64) - wm))
+    measured = loss(wp) - loss(wm)
+    assert abs(measured - predicted) <= 1e-2 * abs(predicted), (measured, predicted)
+
+
 def test_short_training_beats_plain_fdk():
     """A few Adam steps on a handful of small noisy scans already lower the volume error below the
     plain Hann-ramp reconstruction of the same scans."""
