@@ -21,6 +21,7 @@ ERRORS = {
     -5: "FDK_ERR_UNSUPPORTED",
     -6: "FDK_ERR_NO_DEVICE",
     -7: "FDK_ERR_DEVICE_CHECK",
+    -8: "FDK_ERR_IO",
 }
 
 # filter windows (s_FILTER_TYPE order, common/type.h:4619-4626)
@@ -34,17 +35,20 @@ PRECISIONS = {"fp32_exact": BP_FP32_EXACT, "fp32": BP_FP32, "mixed": BP_MIXED}
 EXPORTED = [
     "fdk_last_error", "fdk_abi_version", "fdk_device_count",
     "fdk_geometry_default", "fdk_filter_length", "fdk_filter_design", "fdk_angular_ramp_factor",
-    "fdk_cos_table", "fdk_view_angles", "fdk_projection_matrices",
+    "fdk_cos_table", "fdk_csc_table", "fdk_view_angles", "fdk_projection_matrices",
     "fdk_filter_create", "fdk_filter_filtering", "fdk_filter_run_device", "fdk_filter_destroy",
     "fdk_correct_image_real32", "fdk_filter_row_real32", "fdk_filter_row_real32_noalloc",
     "fdk_bp_create", "fdk_bp_bp", "fdk_bp_bp_device", "fdk_bp_get_volume", "fdk_bp_volume_device",
     "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
     "fdk_rtk_reconstruct_conebeam",
-    "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device", "fdk_recon_sync",
+    "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device",
+    "fdk_recon_push_folder", "fdk_recon_sync",
     "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_reset", "fdk_recon_destroy",
     "fdk_phantom_project", "fdk_forward_project", "fdk_probe_smem", "fdk_probe_fma",
     "fdk_nn_param_count", "fdk_nn_forward", "fdk_nn_backward", "fdk_adam_step", "fdk_transmission_noise",
     "fdk_voxelize", "fdk_rows_to_mirror", "fdk_volume_mse", "fdk_bp_adjoint",
+    "fdk_proj_path", "fdk_load_proj_folder", "fdk_save_proj_folder", "fdk_save_volume", "fdk_load_volume",
+    "fdk_save_volume_slices",
 ]
 
 
@@ -104,6 +108,7 @@ def lib() -> C.CDLL:
         "fdk_filter_design": ([i32, i64, i32, vp, i64], C.c_int),
         "fdk_angular_ramp_factor": ([G, f64p], C.c_int),
         "fdk_cos_table": ([G, vp], C.c_int),
+        "fdk_csc_table": ([G, vp], C.c_int),
         "fdk_view_angles": ([G, vp], C.c_int),
         "fdk_projection_matrices": ([G, vp, vp], C.c_int),
         "fdk_filter_create": ([C.POINTER(vp), vp, vp, i64, i64, i64, i32, i32], C.c_int),
@@ -128,6 +133,7 @@ def lib() -> C.CDLL:
         "fdk_recon_stream": ([vp, C.POINTER(vp)], C.c_int),
         "fdk_recon_push": ([vp, vp, i64, i64], C.c_int),
         "fdk_recon_push_device": ([vp, vp, i64, i64], C.c_int),
+        "fdk_recon_push_folder": ([vp, C.c_char_p, i64, i64, i32, i32, i32], C.c_int),
         "fdk_recon_sync": ([vp, i64], C.c_int),
         "fdk_recon_get_volume": ([vp, vp, i64], C.c_int),
         "fdk_recon_stats": ([vp, f64p, f64p, C.POINTER(i64)], C.c_int),
@@ -144,6 +150,12 @@ def lib() -> C.CDLL:
         "fdk_rows_to_mirror": ([vp, vp, i64, i32, i32, vp], C.c_int),
         "fdk_volume_mse": ([vp, vp, vp, i32, i32, i32, f64p, vp], C.c_int),
         "fdk_bp_adjoint": ([G, vp, vp, i32, vp, vp], C.c_int),
+        "fdk_proj_path": ([C.c_char_p, i64, i32, i32, C.c_char_p, i32], C.c_int),
+        "fdk_load_proj_folder": ([C.c_char_p, i32, i32, i64, i64, i32, i32, vp, i32], C.c_int),
+        "fdk_save_proj_folder": ([C.c_char_p, vp, i32, i32, i64, i64, i32, i32], C.c_int),
+        "fdk_save_volume": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
+        "fdk_load_volume": ([C.c_char_p, vp, i64, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
+        "fdk_save_volume_slices": ([C.c_char_p, vp, i32, i32, i32, i32, i32], C.c_int),
         "fdk_probe_smem": ([i32, f64p], C.c_int),
         "fdk_probe_fma": ([i32, f64p], C.c_int),
     }

@@ -177,6 +177,16 @@ int fdk_cos_table(const fdk_geometry *g, float *out) {
     FDK_ABI_END
 }
 
+// csc_sigma = 1 / cos_sigma, taken of the stored FP32 value in FP64 (common/type.h:4784).
+int fdk_csc_table(const fdk_geometry *g, float *out) {
+    FDK_ABI_BEGIN
+    FDK_TRY(fdk_cos_table(g, out));
+    const int64_t n = g->nu * g->nv;
+    for (int64_t i = 0; i < n; i++) out[i] = (float)(1.0 / (double)out[i]);
+    return FDK_OK;
+    FDK_ABI_END
+}
+
 int fdk_view_angles(const fdk_geometry *g, double *out) {
     FDK_ABI_BEGIN
     FDK_TRY(check_geometry(g));

@@ -1,5 +1,7 @@
 // internal.h -- declarations shared between translation units of libfdk_b200.
 #pragma once
+#include <string>
+
 #include "common.h"
 
 namespace fdk {
@@ -21,5 +23,11 @@ int filter_views(const float *src, int src_pitch, long long src_vstride, void *d
                  long long dst_vstride, const float *cos, int cos_pitch, const FilterTables &t, int nu, int nv,
                  int pad_n, int n_views, int layout, int dtype, cudaStream_t st, float out_scale = 1.0f,
                  unsigned int *overflow = nullptr);
+
+// Projection-folder files (io.cpp): folder + "img%04d.raw" % file_index, and count views
+// (files (first + i) * step + start, sizes checked first) read by `threads` host threads.
+std::string proj_file_path(const char *folder, long long file_index);
+int read_views(const char *folder, int nu, int nv, long long first, long long count, int step, int start, float *dst,
+               int threads);
 
 }  // namespace fdk

@@ -44,6 +44,9 @@ struct fdk_recon {
     double filter_ms = 0;
     long long views = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
+    // pinned staging of fdk_recon_push_folder (allocated on first use): two batches
+    float *h_stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};
 };
 
 // internal hooks (bp.cu)
@@ -61,6 +64,8 @@ int recon_release(fdk_recon *h) {
     if (h->bp) fdk_bp_destroy(h->bp);
     h->tables.release();
     for (int i = 0; i < 2; i++) {
+        if (h->h_stage[i]) cudaFreeHost(h->h_stage[i]);
+        if (h->stage_free[i]) cudaEventDestroy(h->stage_free[i]);
         if (h->d_raw[i]) cudaFree(h->d_raw[i]);
         if (h->raw_ready[i]) cudaEventDestroy(h->raw_ready[i]);
         if (h->raw_free[i]) cudaEventDestroy(h->raw_free[i]);
@@ -237,6 +242,61 @@ int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t
     }
     // the caller may reuse host_views once its last copy has landed
     if (last) FDK_CUDA(cudaEventSynchronize(last));
+    return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64_t n, int32_t step, int32_t start,
+                          int32_t threads) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && folder, "NULL argument");
+    FDK_CHECK_ARG(first >= 0 && n > 0 && first + n <= h->g.n_proj, "view range [%lld, %lld) outside 0..%lld",
+                  (long long)first, (long long)(first + n), (long long)h->g.n_proj);
+    FDK_CHECK_ARG(step >= 1 && start >= 0, "step %d / start %d", step, start);
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    const int nu = (int)h->g.nu, nv = (int)h->g.nv;
+    const long long frame = (long long)nu * nv;
+    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    // sizes of every file first, as the reference's folder loader
+    for (long long i = 0; i < n; i++) {
+        const std::string p = proj_file_path(folder, (first + i) * step + start);
+        FILE *fp = std::fopen(p.c_str(), "rb");
+        long long sz = -1;
+        if (fp) {
+            std::fseek(fp, 0, SEEK_END);
+            sz = std::ftell(fp);
+            std::fclose(fp);
+        }
+        if (sz != frame * (long long)sizeof(float)) {
+            set_error("%s: %s (expected %lld bytes of FP32, %d x %d)", p.c_str(), sz < 0 ? "missing" : "wrong size",
+                      frame * (long long)sizeof(float), nu, nv);
+            return FDK_ERR_IO;
+        }
+    }
+    for (int k = 0; k < 2; k++) {
+        if (!h->h_stage[k]) FDK_CUDA(cudaHostAlloc((void **)&h->h_stage[k], sizeof(float) * frame * cap, 0));
+        if (!h->stage_free[k]) {
+            FDK_CUDA(cudaEventCreateWithFlags(&h->stage_free[k], cudaEventDisableTiming));
+            FDK_CUDA(cudaEventRecord(h->stage_free[k], h->copy));
+        }
+    }
+    int b = 0;
+    for (long long c = 0; c < n; c += cap, b ^= 1) {
+        const int m = (int)std::min<long long>(cap, n - c);
+        FDK_CUDA(cudaEventSynchronize(h->stage_free[b]));  // staging b's previous copy has landed
+        FDK_TRY(read_views(folder, nu, nv, first + c, m, step, start, h->h_stage[b], threads));
+        const int k = h->slot;
+        h->slot ^= 1;
+        FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
+        FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], h->h_stage[b], sizeof(float) * frame * m, cudaMemcpyHostToDevice,
+                                 h->copy));
+        FDK_CUDA(cudaEventRecord(h->stage_free[b], h->copy));
+        FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
+        FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
+        FDK_TRY(process_chunk(h, h->d_raw[k], first + c, m, h->raw_free[k]));
+    }
     return FDK_OK;
     FDK_ABI_END
 }

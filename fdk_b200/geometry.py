@@ -81,6 +81,13 @@ class Parameter:
         return out
 
     @property
+    def csc_sigma(self) -> np.ndarray:
+        """cos_image_table.csc_sigma = 1 / cos_sigma, nv rows x nu (common/type.h:4760, 4784)."""
+        out = np.zeros((self.nv, self.nu), np.float32)
+        check(lib().fdk_csc_table(C.byref(self.to_c()), out.ctypes.data))
+        return out
+
+    @property
     def angles(self) -> np.ndarray:
         """direction * vec_deg / 180 * pi + volume_postion_angle per view (radians)."""
         out = np.zeros(self.nProj, np.float64)

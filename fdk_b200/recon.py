@@ -44,6 +44,11 @@ class Reconstructor:
     def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push(self._h, host_ptr, first, n))
 
+    def push_folder(self, folder: str, first: int, n: int, step: int = 1, start: int = 0, threads: int = 0) -> None:
+        """Views first..first+n-1 from a projection folder (img%04d.raw, view v in file v*step+start),
+        read into pinned staging while the previous batch is copied and reconstructed."""
+        check(lib().fdk_recon_push_folder(self._h, _folder_arg(folder), first, n, step, start, threads))
+
     def push_device(self, dev_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push_device(self._h, dev_ptr, first, n))
 
@@ -81,3 +86,8 @@ class Reconstructor:
             self.close()
         except Exception:
             pass
+
+
+def _folder_arg(folder: str) -> bytes:
+    """The C entry points append file names to the folder string, as the reference does."""
+    return (folder if folder.endswith("/") else folder + "/").encode()

@@ -46,6 +46,7 @@ extern "C" {
 #define FDK_ERR_UNSUPPORTED (-5)   /* valid request this build does not implement */
 #define FDK_ERR_NO_DEVICE (-6)     /* no CUDA device visible */
 #define FDK_ERR_DEVICE_CHECK (-7)  /* a kernel reported an internal check failure */
+#define FDK_ERR_IO (-8)            /* a file could not be opened, read or written, or has the wrong size */
 
 const char *fdk_last_error(void);
 int fdk_abi_version(void);
@@ -89,6 +90,9 @@ int fdk_angular_ramp_factor(const fdk_geometry *g, double *out);
 /* cos_sigma table, nv rows of nu (CalculateCosTable, common/type.h:4756-4783):
  * SID/sqrt(u^2+v^2+SID^2) * SOD^2 * AngularAndrampFactor, FP32 storage. */
 int fdk_cos_table(const fdk_geometry *g, float *out);
+/* csc_sigma table: 1 / cos_sigma of the stored FP32 cos_sigma, in FP64, stored FP32
+ * (common/type.h:4760, 4784). */
+int fdk_csc_table(const fdk_geometry *g, float *out);
 /* Per-view angles in radians: direction*deg/180*pi + volume_position_angle, deg = i*scan_angle/n_proj
  * (common/type.h:4729, 4824). */
 int fdk_view_angles(const fdk_geometry *g, double *out);
@@ -231,6 +235,12 @@ int fdk_recon_stream(fdk_recon *h, void **stream);
 int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t n);
 /* Push n raw views already in device memory (nv x nu each). */
 int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n);
+/* Push views first..first+n-1 from a projection folder (files as fdk_proj_path, view v in file
+ * v * step + start).  Files are read by `threads` host threads (<= 0: up to 8) into two pinned
+ * staging buffers of one batch each, so reading batch k+1 overlaps the copy and the kernels of
+ * batch k.  Every file's size is checked before any is read (FDK_ERR_IO names the first bad one). */
+int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64_t n, int32_t step,
+                          int32_t start, int32_t threads);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
 /* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).
@@ -240,6 +250,28 @@ int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size);
 int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views);
 int fdk_recon_reset(fdk_recon *h);
 int fdk_recon_destroy(fdk_recon *h);
+
+/* ---- on-disk formats (common/type.h, cuFDK/mpiFDK.cpp) ----------------------- */
+/* Path of view `view`'s raw file: folder + "img%04d.raw" % (view * step + start)
+ * (Parameter::GetProjPath, common/type.h:4847-4851; folder carries its trailing '/'). */
+int fdk_proj_path(const char *folder, int64_t view, int32_t step, int32_t start, char *out, int32_t capacity);
+/* Views first..first+count-1 from a projection folder into host_views (count x nv x nu FP32, u
+ * fastest), `threads` readers (<= 0: up to 8).  As LoadProjectionImageFolder (common/type.h:1797-1828)
+ * every file must hold exactly nu * nv FP32 values, checked before any is read. */
+int fdk_load_proj_folder(const char *folder, int32_t nu, int32_t nv, int64_t first, int64_t count, int32_t step,
+                         int32_t start, float *host_views, int32_t threads);
+/* Views to folder + img%04d.raw % ((first + i) * step), creating the folder (SaveToFolder,
+ * common/type.h:3848-3861). */
+int fdk_save_proj_folder(const char *folder, const float *host_views, int32_t nu, int32_t nv, int64_t first,
+                         int64_t count, int32_t step, int32_t threads);
+/* ".vol": int32 nx, ny, nz, then nx*ny*nz FP32 voxels [z][y][x] (VolumeT::Save/Load,
+ * common/type.h:3256-3313).  fdk_load_volume with host_vol NULL only reads the header. */
+int fdk_save_volume(const char *path, const float *host_vol, int32_t nx, int32_t ny, int32_t nz);
+int fdk_load_volume(const char *path, float *host_vol, int64_t capacity, int32_t *nx, int32_t *ny, int32_t *nz);
+/* Slices z0..z0+depth-1 of a [z][y][x] block (host_vol starts at slice z0), one raw FP32 file of
+ * nx*ny per slice named folder + "%06d.raw" % z (the slice writer of cuFDK/mpiFDK.cpp:548-576). */
+int fdk_save_volume_slices(const char *folder, const float *host_vol, int32_t nx, int32_t ny, int32_t z0,
+                           int32_t depth, int32_t threads);
 
 /* ---- synthetic data: analytic ellipsoid projections on the device ---------- */
 /* ell: host, n_ell records of 16 doubles {cx, cy, cz, a, b, c, R00..R22, rho} in the world frame

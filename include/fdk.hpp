@@ -138,6 +138,11 @@ class Reconstructor {
     void PushDevice(const float *dev_views, int64_t first, int64_t n) {
         check(fdk_recon_push_device(h_, dev_views, first, n));
     }
+    // views first..first+n-1 from a projection folder (folder + "img%04d.raw", file v*step+start)
+    void PushFolder(const std::string &folder, int64_t first, int64_t n, int step = 1, int start = 0,
+                    int threads = 0) {
+        check(fdk_recon_push_folder(h_, folder.c_str(), first, n, step, start, threads));
+    }
     void Sync(int64_t timeout_ms = 0) { check(fdk_recon_sync(h_, timeout_ms)); }
     void GetVolume(float *host_vol, int64_t size) { check(fdk_recon_get_volume(h_, host_vol, size)); }
     fdk_recon *handle() { return h_; }
@@ -145,5 +150,35 @@ class Reconstructor {
   private:
     fdk_recon *h_ = nullptr;
 };
+
+// On-disk formats (common/type.h): projection folders of img%04d.raw, ".vol" volumes, slice files.
+inline std::string GetProjPath(const std::string &folder, int64_t view, int step = 1, int start = 0) {
+    char buf[4096];
+    check(fdk_proj_path(folder.c_str(), view, step, start, buf, (int32_t)sizeof(buf)));
+    return buf;
+}
+inline void LoadProjectionFolder(const std::string &folder, int nu, int nv, int64_t first, int64_t count,
+                                 float *host_views, int step = 1, int start = 0, int threads = 0) {
+    check(fdk_load_proj_folder(folder.c_str(), nu, nv, first, count, step, start, host_views, threads));
+}
+inline void SaveProjectionFolder(const std::string &folder, const float *host_views, int nu, int nv, int64_t first,
+                                 int64_t count, int step = 1, int threads = 0) {
+    check(fdk_save_proj_folder(folder.c_str(), host_views, nu, nv, first, count, step, threads));
+}
+inline void SaveVolume(const std::string &path, const float *vol, int nx, int ny, int nz) {
+    check(fdk_save_volume(path.c_str(), vol, nx, ny, nz));
+}
+inline std::vector<float> LoadVolume(const std::string &path, int &nx, int &ny, int &nz) {
+    int32_t x = 0, y = 0, z = 0;
+    check(fdk_load_volume(path.c_str(), nullptr, 0, &x, &y, &z));
+    std::vector<float> v((size_t)x * y * z);
+    check(fdk_load_volume(path.c_str(), v.data(), (int64_t)v.size(), &x, &y, &z));
+    nx = x, ny = y, nz = z;
+    return v;
+}
+inline void SaveVolumeSlices(const std::string &folder, const float *vol, int nx, int ny, int z0, int depth,
+                             int threads = 0) {
+    check(fdk_save_volume_slices(folder.c_str(), vol, nx, ny, z0, depth, threads));
+}
 
 }  // namespace fdk
