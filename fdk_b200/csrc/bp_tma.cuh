@@ -35,21 +35,37 @@ namespace fdk {
 
 template <typename E>
 struct TmaCfg;
+// Tile and pipeline shape of the mixed-precision kernel; the macros exist for tuning sweeps.
+#ifndef FDK_TMA_MIXED_R
+#define FDK_TMA_MIXED_R 12
+#endif
+#ifndef FDK_TMA_MIXED_S
+#define FDK_TMA_MIXED_S 3
+#endif
+#ifndef FDK_TMA_MIXED_NV
+#define FDK_TMA_MIXED_NV 4
+#endif
 template <>
 struct TmaCfg<__half2> {
-    static constexpr int R = 12;   // top-slab slices per thread
-    static constexpr int BW = 36;  // box width (v elements), 144 B rows
-    static constexpr int BH = 40;  // box height (u rows)
-    static constexpr int NV = 4;   // views per stage
-    static constexpr int S = 3;    // stages
+    static constexpr int R = FDK_TMA_MIXED_R;    // top-slab slices per thread
+    static constexpr int BW = 36;                // box width (v elements), 144 B rows
+    static constexpr int BH = 40;                // box height (u rows)
+    static constexpr int NV = FDK_TMA_MIXED_NV;  // views per stage
+    static constexpr int S = FDK_TMA_MIXED_S;    // stages
 };
+#ifndef FDK_TMA_FP32_R
+#define FDK_TMA_FP32_R 8
+#endif
+#ifndef FDK_TMA_FP32_S
+#define FDK_TMA_FP32_S 2
+#endif
 template <>
 struct TmaCfg<float2> {
-    static constexpr int R = 8;
+    static constexpr int R = FDK_TMA_FP32_R;
     static constexpr int BW = 34;  // 272 B rows
     static constexpr int BH = 40;
     static constexpr int NV = 4;
-    static constexpr int S = 2;
+    static constexpr int S = FDK_TMA_FP32_S;
 };
 
 constexpr long long kWaitLimit = 1ll << 26;

@@ -18,6 +18,8 @@ learned reconstruction is kept only when its error against the phantom is lower.
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
+import math
 import time
 
 import numpy as np
@@ -52,9 +54,13 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 class Pipeline:
-    """Device buffers and kernels for one scan geometry (torch for device memory only)."""
+    """Device buffers and kernels for one scan geometry (torch for device memory only).
 
-    def __init__(self, param=None, device: int = 0):
+    input_window: the ramp-filter window of the rows the network reads ("hann", the geometry's
+    own, or e.g. "ram-lak" to let the network learn its own apodization).  Plain FDK, the
+    fallback and judge, always uses the geometry's window."""
+
+    def __init__(self, param=None, device: int = 0, input_window: str | None = None):
         import torch
 
         self.torch = torch
@@ -76,12 +82,19 @@ class Pipeline:
         self.mats_h = p.proj_matrices()
         self.mats_d = torch.from_numpy(self.mats_h.reshape(-1)).to(self.dev)
         self.engine = FilterEngine(p.cos_sigma, p.fft_kernel_real_f32, pad_edge=4, device=device)
+        self.input_window = input_window or p.str_filter
+        if self.input_window != p.str_filter:
+            q = dataclasses.replace(p, str_filter=self.input_window)
+            self.engine_in = FilterEngine(p.cos_sigma, q.fft_kernel_real_f32, pad_edge=4, device=device)
+        else:
+            self.engine_in = self.engine
         self.bp = BackProjectionFDK(p.nv, p.nu, 128, p.nx, p.ny, p.nz, BoxT(0, 0, 0, p.nx, p.ny, p.nz // 2),
                                     BoxT(0, 0, p.nz // 2, p.nx, p.ny, p.nz // 2), "fp32", device)
 
     # ------------------------------------------------------------------ data
-    def scan(self, seed: int, out_rows) -> np.ndarray:
-        """Phantom `seed`: truth -> self.truth, noisy filtered rows -> out_rows.  Returns ellipsoids."""
+    def scan(self, seed: int, out_rows, plain_rows=None) -> np.ndarray:
+        """Phantom `seed`: truth -> self.truth, the noisy views filtered with the input window ->
+        out_rows, and with the geometry's window -> plain_rows (if given).  Returns ellipsoids."""
         p = self.p
         rng = np.random.default_rng(seed)
         ell = random_ellipsoids(seed, int(rng.integers(10, 31)), 0.5 * p.nx * p.dx)
@@ -91,7 +104,11 @@ class Pipeline:
                                         None))
         check(lib().fdk_transmission_noise(self.proj.data_ptr(), self.proj.numel(), I0, MU,
                                            np.uint64(seed * 7919 + 17), None))
-        self.engine.run_device(self.proj.data_ptr(), out_rows.data_ptr(), p.nProj, _lib.LAYOUT_ROWS, _lib.DTYPE_F32)
+        self.engine_in.run_device(self.proj.data_ptr(), out_rows.data_ptr(), p.nProj, _lib.LAYOUT_ROWS,
+                                  _lib.DTYPE_F32)
+        if plain_rows is not None:
+            self.engine.run_device(self.proj.data_ptr(), plain_rows.data_ptr(), p.nProj, _lib.LAYOUT_ROWS,
+                                   _lib.DTYPE_F32)
         return ell
 
     def truth_of(self, seed: int):
@@ -133,12 +150,14 @@ class Pipeline:
 
 
 def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 1000, params=None, log=print,
-          time_limit_s: float | None = None, on_epoch=None) -> dict:
+          time_limit_s: float | None = None, on_epoch=None, schedule: str = "constant",
+          input_window: str | None = None) -> dict:
     """Adam on volume MSE, one phantom per step; the training scans are generated once.
+    schedule: "constant" (lr throughout) or "cosine" (lr decayed to lr/100 over all steps).
     on_epoch(epoch, params, history), when given, runs after every epoch (checkpointing)."""
     import torch
 
-    pl = Pipeline()
+    pl = Pipeline(input_window=input_window)
     p = pl.p
     xs = torch.empty((n_train, p.nProj, p.nv, p.nu), dtype=torch.float32, device=pl.dev)
     t0 = time.time()
@@ -150,6 +169,7 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
     m = torch.zeros_like(w)
     v = torch.zeros_like(w)
     hist, step, t0 = [], 0, time.time()
+    total = n_train * epochs
     rng = np.random.default_rng(7)
     stopped = False
     for ep in range(epochs):
@@ -161,8 +181,9 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
             tot += pl.mse(with_grad=True)
             pl.gradient(w, xs[i])
             step += 1
-            check(lib().fdk_adam_step(w.data_ptr(), pl.dparams.data_ptr(), m.data_ptr(), v.data_ptr(), w.numel(), lr,
-                                      0.9, 0.999, 1e-8, step, None))
+            lr_t = lr if schedule == "constant" else lr * (0.01 + 0.99 * 0.5 * (1 + math.cos(math.pi * step / total)))
+            check(lib().fdk_adam_step(w.data_ptr(), pl.dparams.data_ptr(), m.data_ptr(), v.data_ptr(), w.numel(),
+                                      lr_t, 0.9, 0.999, 1e-8, step, None))
             if time_limit_s is not None and time.time() - t0 > time_limit_s:
                 stopped = True
                 break
@@ -178,18 +199,19 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
             "epochs_completed": len(hist) if not stopped else len(hist) - 1, "stopped_early": stopped}
 
 
-def evaluate(params, n_test: int = 200, seed0: int = 5000) -> dict:
+def evaluate(params, n_test: int = 200, seed0: int = 5000, input_window: str | None = None) -> dict:
     """Held-out scans: MSE of plain FDK, of the learned filter, and of the judged choice."""
     import torch
 
-    pl = Pipeline()
+    pl = Pipeline(input_window=input_window)
     p = pl.p
     x = torch.empty((p.nProj, p.nv, p.nu), dtype=torch.float32, device=pl.dev)
+    xp = torch.empty_like(x) if pl.engine_in is not pl.engine else x
     w = torch.from_numpy(np.asarray(params, np.float32)).to(pl.dev)
     plain, learned, kept = [], [], []
     for i in range(n_test):
-        pl.scan(seed0 + i, x)
-        pl.reconstruct(None, x)
+        pl.scan(seed0 + i, x, xp if xp is not x else None)
+        pl.reconstruct(None, xp)
         e0 = pl.mse(with_grad=False)
         pl.reconstruct(w, x)
         e1 = pl.mse(with_grad=False)

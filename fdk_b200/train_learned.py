@@ -29,6 +29,8 @@ def main():
     ap.add_argument("--n-test", type=int, default=200)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--time-limit", type=float, default=None, help="stop training after this many seconds")
+    ap.add_argument("--schedule", default="constant", choices=["constant", "cosine"])
+    ap.add_argument("--input-window", default=None, help="ramp window of the network's input rows (default: hann)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                   "residual_c5.npz"))
     args = ap.parse_args()
@@ -36,13 +38,18 @@ def main():
     t0 = time.time()
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
 
-    def checkpoint(ep, params, hist):
-        np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * args.n_train)
+    window = args.input_window or "hann"
 
-    tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit, on_epoch=checkpoint)
-    np.savez(args.out, params=tr["params"], history=np.asarray(tr["history"]), steps=tr["steps"])
-    ev = learned.evaluate(tr["params"], args.n_test)
+    def checkpoint(ep, params, hist):
+        np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * args.n_train,
+                 input_window=window)
+
+    tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit, on_epoch=checkpoint,
+                       schedule=args.schedule, input_window=args.input_window)
+    np.savez(args.out, params=tr["params"], history=np.asarray(tr["history"]), steps=tr["steps"], input_window=window)
+    ev = learned.evaluate(tr["params"], args.n_test, input_window=args.input_window)
     out = {"workload": "C5: 256^3, 90 views of 256^2, I0=1e4, mu=0.02/mm", "n_train": args.n_train,
+           "schedule": args.schedule, "input_window": window, "lr": args.lr,
            "epochs_requested": args.epochs, "epochs_run": len(tr["history"]), "steps": tr["steps"],
            "stopped_early": tr["stopped_early"], "train_seconds": tr["seconds"], "history": tr["history"],
            "eval": ev, "total_seconds": time.time() - t0, "weights": os.path.relpath(args.out)}
