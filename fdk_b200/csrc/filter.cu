@@ -9,8 +9,16 @@
 // CTA emit the backprojection's mirror-pair layout directly.
 //
 // FFT: radix-2 decimation in frequency (natural -> bit-reversed order), pointwise multiply by
-// H[bitrev(p)]/W, radix-2 decimation in time (bit-reversed -> natural), all in shared memory.
-// Twiddles come from an FP64-computed table.
+// H[bitrev(p)]/W, radix-2 decimation in time (bit-reversed -> natural), in shared memory.
+// Three consecutive radix-2 stages run per pass in registers: the stages of a pass touch three
+// adjacent index bits, so the 8 elements that differ only in those bits form a closed group.
+// Every butterfly is the plain radix-2 one, so the arithmetic is that of the stage-by-stage
+// transform, with a third of the shared-memory round trips and barriers.  Twiddles come from
+// an FP64-computed table.
+//
+// The backprojection's MIRROR layout is written by filter_mirror_kernel: a CTA filters G row
+// pairs in turn, collects their outputs as an nu x G tile per side in shared memory, and writes
+// each detector column's G consecutive elements as one 16-byte store.
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -60,6 +68,94 @@ __device__ __forceinline__ float row_sample(const FilterArgs &a, const float *vi
     return x;
 }
 
+// One pass of NS consecutive radix-2 DIF stages, the first being stage s0 (half = W >> (s0+1)).
+// Those stages touch index bits hbit .. hbit-NS+1; a group is the 2^NS elements that differ only
+// there.  Butterfly: (x, y) -> (x + y, (x - y) tw[(i & (half-1)) << stage]).  hb_tab (last pass
+// only) multiplies the bit-reversed result by H[bitrev(p)] / W.
+template <int NS>
+__device__ __forceinline__ void dif_pass(float2 *buf, const float2 *__restrict__ tw, const float *__restrict__ hb_tab,
+                                         int W, int log2W, int s0) {
+    constexpr int GS = 1 << NS;
+    const int hbit = log2W - 1 - s0;
+    const int low = hbit - NS + 1;
+    for (int g = threadIdx.x; g < (W >> NS); g += blockDim.x) {
+        const int base = ((g >> low) << (hbit + 1)) | (g & ((1 << low) - 1));
+        float2 v[GS];
+#pragma unroll
+        for (int j = 0; j < GS; j++) v[j] = buf[base + (j << low)];
+#pragma unroll
+        for (int t = 0; t < NS; t++) {
+            const int hstep = GS >> (t + 1);
+            const int half = 1 << (hbit - t);
+#pragma unroll
+            for (int j = 0; j < GS; j++) {
+                if (j & hstep) continue;
+                const int i0 = base + (j << low);
+                const float2 x = v[j], y = v[j + hstep];
+                v[j] = make_float2(x.x + y.x, x.y + y.y);
+                v[j + hstep] = cmul(make_float2(x.x - y.x, x.y - y.y), __ldg(tw + ((i0 & (half - 1)) << (s0 + t))));
+            }
+        }
+        if (hb_tab) {
+#pragma unroll
+            for (int j = 0; j < GS; j++) {
+                const float h = __ldg(hb_tab + base + (j << low));
+                v[j] = make_float2(v[j].x * h, v[j].y * h);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < GS; j++) buf[base + (j << low)] = v[j];
+    }
+}
+
+// One pass of NS consecutive radix-2 DIT stages on index bits b0 .. b0+NS-1 (half = 2^b0 first).
+// Butterfly: t = y conj(tw[(i & (half-1)) * W / (2 half)]); (x, y) -> (x + t, x - t).
+template <int NS>
+__device__ __forceinline__ void dit_pass(float2 *buf, const float2 *__restrict__ tw, int W, int log2W, int b0) {
+    constexpr int GS = 1 << NS;
+    for (int g = threadIdx.x; g < (W >> NS); g += blockDim.x) {
+        const int base = ((g >> b0) << (b0 + NS)) | (g & ((1 << b0) - 1));
+        float2 v[GS];
+#pragma unroll
+        for (int j = 0; j < GS; j++) v[j] = buf[base + (j << b0)];
+#pragma unroll
+        for (int t = 0; t < NS; t++) {
+            const int hstep = 1 << t;
+            const int half = 1 << (b0 + t);
+#pragma unroll
+            for (int j = 0; j < GS; j++) {
+                if (j & hstep) continue;
+                const int i0 = base + (j << b0);
+                const float2 x = v[j];
+                const float2 u = cmulc(v[j + hstep], __ldg(tw + ((i0 & (half - 1)) << (log2W - 1 - b0 - t))));
+                v[j] = make_float2(x.x + u.x, x.y + u.y);
+                v[j + hstep] = make_float2(x.x - u.x, x.y - u.y);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < GS; j++) buf[base + (j << b0)] = v[j];
+    }
+}
+
+// Forward transform, multiply by H, inverse transform of buf (W points); ends after a barrier.
+__device__ __forceinline__ void filter_fft(float2 *buf, const FilterArgs &a) {
+    for (int s = 0; s < a.log2W; s += 3) {
+        const int ns = min(3, a.log2W - s);
+        const float *h = (s + ns == a.log2W) ? a.hb : nullptr;
+        if (ns == 3) dif_pass<3>(buf, a.tw, h, a.W, a.log2W, s);
+        else if (ns == 2) dif_pass<2>(buf, a.tw, h, a.W, a.log2W, s);
+        else dif_pass<1>(buf, a.tw, h, a.W, a.log2W, s);
+        __syncthreads();
+    }
+    for (int b = 0; b < a.log2W; b += 3) {
+        const int ns = min(3, a.log2W - b);
+        if (ns == 3) dit_pass<3>(buf, a.tw, a.W, a.log2W, b);
+        else if (ns == 2) dit_pass<2>(buf, a.tw, a.W, a.log2W, b);
+        else dit_pass<1>(buf, a.tw, a.W, a.log2W, b);
+        __syncthreads();
+    }
+}
+
 // Mean of the first (or last) pad_n weighted samples of row r.
 __device__ float edge_mean(const FilterArgs &a, const float *view, int r, bool left) {
     float s = 0.f;
@@ -98,37 +194,7 @@ __global__ void __launch_bounds__(256) filter_rows_kernel(FilterArgs a) {
     }
     __syncthreads();
 
-    // forward: decimation in frequency
-    for (int half = W >> 1, step = 1; half >= 1; half >>= 1, step <<= 1) {
-        for (int b = threadIdx.x; b < (W >> 1); b += blockDim.x) {
-            const int j = b & (half - 1);
-            const int i0 = ((b - j) << 1) + j;
-            const int i1 = i0 + half;
-            const float2 x = buf[i0], y = buf[i1];
-            buf[i0] = make_float2(x.x + y.x, x.y + y.y);
-            buf[i1] = cmul(make_float2(x.x - y.x, x.y - y.y), __ldg(a.tw + j * step));
-        }
-        __syncthreads();
-    }
-    for (int k = threadIdx.x; k < W; k += blockDim.x) {
-        const float h = __ldg(a.hb + k);
-        float2 v = buf[k];
-        buf[k] = make_float2(v.x * h, v.y * h);
-    }
-    __syncthreads();
-    // inverse: decimation in time, conjugate twiddles
-    for (int half = 1, step = W >> 1; half < W; half <<= 1, step >>= 1) {
-        for (int b = threadIdx.x; b < (W >> 1); b += blockDim.x) {
-            const int j = b & (half - 1);
-            const int i0 = ((b - j) << 1) + j;
-            const int i1 = i0 + half;
-            const float2 x = buf[i0];
-            const float2 t = cmulc(buf[i1], __ldg(a.tw + j * step));
-            buf[i0] = make_float2(x.x + t.x, x.y + t.y);
-            buf[i1] = make_float2(x.x - t.x, x.y - t.y);
-        }
-        __syncthreads();
-    }
+    filter_fft(buf, a);
 
     OUT *dst = reinterpret_cast<OUT *>(a.dst);
     for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
@@ -151,6 +217,68 @@ __global__ void __launch_bounds__(256) filter_rows_kernel(FilterArgs a) {
                 d[2 * r2 + 1] = o1;
             }
         }
+    }
+}
+
+template <typename OUT>
+struct PairOf;
+template <>
+struct PairOf<float> {
+    using T = float2;
+    static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
+};
+template <>
+struct PairOf<__half> {
+    using T = __half2;
+    static __device__ __forceinline__ T make(__half a, __half b) { return __halves2half2(a, b); }
+};
+
+// MIRROR layout, G row pairs (r, nv-1-r), r = G * blockIdx.x + g, per CTA; G * sizeof(pair) = 16.
+template <typename OUT, int G>
+__global__ void __launch_bounds__(512) filter_mirror_kernel(FilterArgs a) {
+    using P = typename PairOf<OUT>::T;
+    static_assert(G * sizeof(P) == 16, "one 16-byte store per column and side");
+    extern __shared__ __align__(16) unsigned char fsm[];
+    float2 *buf = reinterpret_cast<float2 *>(fsm);
+    P *stg = reinterpret_cast<P *>(fsm + sizeof(float2) * a.W);  // [side][u][G]
+    __shared__ float pads[4];
+    const int view = blockIdx.y, r0 = blockIdx.x * G;
+    const float *vsrc = a.src + (long long)view * a.src_vstride;
+    for (int g = 0; g < G; g++) {
+        const int r1 = r0 + g, r2 = a.nv - 1 - r1;
+        if (threadIdx.x < 4) pads[threadIdx.x] = edge_mean(a, vsrc, threadIdx.x < 2 ? r1 : r2, (threadIdx.x & 1) == 0);
+        __syncthreads();  // also ends the previous pair's reads of buf
+        for (int k = threadIdx.x; k < a.W; k += blockDim.x) {
+            const int c = k - a.off;
+            float x1, x2;
+            if (c < 0) {
+                x1 = pads[0];
+                x2 = pads[2];
+            } else if (c >= a.nu) {
+                x1 = pads[1];
+                x2 = pads[3];
+            } else {
+                x1 = row_sample(a, vsrc, r1, c);
+                x2 = row_sample(a, vsrc, r2, c);
+            }
+            buf[k] = make_float2(x1, x2);
+        }
+        __syncthreads();
+        filter_fft(buf, a);
+        for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
+            const float2 y = buf[a.off + u];
+            const OUT o1 = to_out<OUT>(a, y.x), o2 = to_out<OUT>(a, y.y);
+            stg[u * G + g] = PairOf<OUT>::make(o1, o2);                     // element (u, r1)
+            stg[(a.nu + u) * G + (G - 1 - g)] = PairOf<OUT>::make(o2, o1);  // element (u, r2)
+        }
+    }
+    __syncthreads();
+    // side 0: elements v = r0 .. r0+G-1; side 1: v = nv-r0-G .. nv-1-r0 (the mirrors, ascending)
+    P *dst = reinterpret_cast<P *>(a.dst) + (long long)view * (a.dst_vstride / 2);
+    for (int i = threadIdx.x; i < 2 * a.nu; i += blockDim.x) {
+        const int side = i >= a.nu, u = side ? i - a.nu : i;
+        const int v0 = side ? a.nv - r0 - G : r0;
+        *reinterpret_cast<uint4 *>(dst + (long long)u * a.dst_pitch + v0) = *reinterpret_cast<const uint4 *>(stg + i * G);
     }
 }
 
@@ -184,21 +312,40 @@ void FilterTables::release() {
     hb = nullptr;
 }
 
+template <typename OUT, int G>
+static int launch_mirror(const FilterArgs &a, int n_views, cudaStream_t st) {
+    using P = typename PairOf<OUT>::T;
+    const size_t smem = sizeof(float2) * a.W + 2 * sizeof(P) * G * a.nu;
+    if (smem > 48 * 1024)  // per device and size: cheap, so set on every launch
+        FDK_CUDA(cudaFuncSetAttribute(filter_mirror_kernel<OUT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    filter_mirror_kernel<OUT, G><<<dim3(a.nv / (2 * G), n_views), 512, smem, st>>>(a);
+    FDK_CUDA(cudaGetLastError());
+    return FDK_OK;
+}
+
 static int launch_filter(const FilterArgs &a, int n_views, int layout, int dtype, cudaStream_t st) {
+    if (layout == FDK_LAYOUT_MIRROR) {
+        // grouped kernel when G pairs tile the rows and every 16-byte store is aligned
+        const int G = dtype == FDK_DTYPE_F32 ? 2 : 4;
+        const size_t pair = dtype == FDK_DTYPE_F32 ? 8 : 4;
+        const size_t smem = sizeof(float2) * a.W + 2 * pair * G * a.nu;
+        if (a.nv % (2 * G) == 0 && ((uintptr_t)a.dst & 15) == 0 && (a.dst_pitch * pair) % 16 == 0 &&
+            (a.dst_vstride * (pair / 2)) % 16 == 0 && smem <= 200 * 1024) {
+            if (dtype == FDK_DTYPE_F32) return launch_mirror<float, 2>(a, n_views, st);
+            return launch_mirror<__half, 4>(a, n_views, st);
+        }
+    }
     const dim3 grid((a.nv + 1) / 2, n_views);
     const size_t smem = sizeof(float2) * a.W;
     if (smem > 48 * 1024) {
-        // opt in to more than 48 KB of dynamic shared memory for every instantiation used
-        static bool done = false;
-        if (!done) {
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-            done = true;
-        }
+        // opt in to more than 48 KB of dynamic shared memory (per device: set on every launch)
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_MIRROR, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     }
 #define FDK_LAUNCH(L, T) filter_rows_kernel<L, T><<<grid, 256, smem, st>>>(a)
     if (dtype == FDK_DTYPE_F32) {

@@ -13,7 +13,7 @@ from ._lib import PRECISIONS, check, lib
 
 
 class Reconstructor:
-    def __init__(self, param, precision: str = "mixed", batch: int = 32, device: int = 0, slab=None):
+    def __init__(self, param, precision: str = "mixed", batch: int = 128, device: int = 0, slab=None):
         self.param = param
         self.precision = precision
         self._g = param.to_c()

@@ -29,7 +29,7 @@ def main():
     ap.add_argument("--n-test", type=int, default=200)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--time-limit", type=float, default=None, help="stop training after this many seconds")
-    ap.add_argument("--schedule", default="constant", choices=["constant", "cosine"])
+    ap.add_argument("--schedule", default="cosine", choices=["constant", "cosine"])
     ap.add_argument("--input-window", default=None, help="ramp window of the network's input rows (default: hann)")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                   "residual_c5.npz"))

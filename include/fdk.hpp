@@ -125,7 +125,7 @@ inline void CUDA_reconstruct_conebeam(int proj_size[3], int vol_size[3], const f
 // Single-GPU streaming FDK (filter -> BP handoff of cuFDK), whole volume or one slab pair.
 class Reconstructor {
   public:
-    Reconstructor(const fdk_geometry &g, int precision = FDK_BP_MIXED, int batch = 32, int device = 0) {
+    Reconstructor(const fdk_geometry &g, int precision = FDK_BP_MIXED, int batch = 128, int device = 0) {
         check(fdk_recon_create(&h_, &g, precision, batch, device));
     }
     Reconstructor(const fdk_geometry &g, int64_t top_z, int64_t depth, int precision, int batch, int device) {

@@ -28,22 +28,26 @@ def test_filter_engine_vs_oracle(nu, nv, transpose):
     assert max_rel(dst, want) <= 2e-6, max_rel(dst, want)
 
 
-def test_device_layouts():
+@pytest.mark.parametrize("nu,nv", [(80, 64), (96, 50), (2048, 16), (300, 24)])
+def test_device_layouts(nu, nv):
+    """All device layouts against the FP64 oracle and each other.  nv = 64 and 16 take the grouped
+    MIRROR kernel (row pairs tiled 2 or 4 at a time), nv = 50 the per-pair fallback, nv = 24 the
+    grouped FP32 and fallback FP16 kernels."""
     import torch
 
-    p = small_param(64, 80, 64, 6)
+    p = small_param(64, nu, nv, 6)
     _, proj = phantom_views(p)
     eng = F.FilterEngine(p.cos_sigma, p.fft_kernel_real_f32)
     src = torch.from_numpy(proj).cuda()
     want = np.stack([O.filter_view(v, p.fft_kernel_real, p.cos_sigma, pad_n=4, transpose=True) for v in proj])
-    t = torch.empty((6, 80, 64), dtype=torch.float32, device="cuda")
+    t = torch.empty((6, nu, nv), dtype=torch.float32, device="cuda")
     eng.run_device(src.data_ptr(), t.data_ptr(), 6, F.LAYOUT_TRANSPOSED, F.DTYPE_F32)
-    m = torch.empty((6, 80, 64, 2), dtype=torch.float32, device="cuda")
+    m = torch.empty((6, nu, nv, 2), dtype=torch.float32, device="cuda")
     eng.run_device(src.data_ptr(), m.data_ptr(), 6, F.LAYOUT_MIRROR, F.DTYPE_F32)
-    h = torch.empty((6, 80, 64, 2), dtype=torch.float16, device="cuda")
+    h = torch.empty((6, nu, nv, 2), dtype=torch.float16, device="cuda")
     scale = float(1.0 / p.cos_sigma.max())  # back to line-integral units, inside the FP16 range
     eng.run_device(src.data_ptr(), h.data_ptr(), 6, F.LAYOUT_MIRROR, F.DTYPE_F16, scale)
-    r = torch.empty((6, 64, 80), dtype=torch.float32, device="cuda")
+    r = torch.empty((6, nv, nu), dtype=torch.float32, device="cuda")
     eng.run_device(src.data_ptr(), r.data_ptr(), 6, F.LAYOUT_ROWS, F.DTYPE_F32)
     torch.cuda.synchronize()
     t, m, h, r = t.cpu().numpy(), m.cpu().numpy(), h.float().cpu().numpy() / scale, r.cpu().numpy()
