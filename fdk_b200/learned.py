@@ -10,7 +10,8 @@ attenuation with mu = 0.02 / mm per unit density (water); the benchmark leaves m
 Training: y = x + net(x) on every cosine-weighted, Hann-ramp-filtered detector row x; the rows go
 to the staged FP32 backprojection; loss = volume MSE against the phantom; the gradient returns
 through the exact backprojection adjoint (fdk_bp_adjoint) and the network's backward kernel;
-Adam (lr 1e-3).  Every kernel is this library's own (learn.cu, fproj.cu, filter.cu, bp_tma.cuh).
+Adam (lr 1e-3, cosine-decayed to 1e-5 over the run by default).  Every kernel is this library's
+own (learn.cu, fproj.cu, filter.cu, bp_tma.cuh).
 
 Plain Hann-ramp FDK (zero residual) is the fallback and the judge: on each held-out scan the
 learned reconstruction is kept only when its error against the phantom is lower.

@@ -2,7 +2,7 @@
 configuration (views and volume larger than L2, a few GB on the device), small enough for
 `ncu --set full -k regex:bp_ -s 1 -c 1`.
 
-  python -m fdk_b200.profile_bp [mixed|fp32|fp32_exact] [n_batches]
+  python -m fdk_b200.profile_bp [mixed|fp32|fp32_exact] [n_batches] [batch]
 """
 import os
 import sys
@@ -15,11 +15,12 @@ from fdk_b200 import phantom as P  # noqa: E402
 
 prec = sys.argv[1] if len(sys.argv) > 1 else "mixed"
 nb = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+B = int(sys.argv[3]) if len(sys.argv) > 3 else 128
 p = F.config("c2")
-views = torch.empty((32 * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
-P.project(p, P.phantom_for(p, 2, 20), 0, 32 * nb, views.data_ptr())
-r = F.Reconstructor(p, prec, batch=32)
+views = torch.empty((B * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
+P.project(p, P.phantom_for(p, 2, 20), 0, B * nb, views.data_ptr())
+r = F.Reconstructor(p, prec, batch=B)
 for b in range(nb):
-    r.push_device(views[32 * b:].data_ptr(), 32 * b, 32)
+    r.push_device(views[B * b:].data_ptr(), B * b, B)
 r.sync()
 print(prec, r.stats())

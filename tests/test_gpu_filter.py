@@ -51,7 +51,8 @@ def test_device_layouts(nu, nv):
     eng.run_device(src.data_ptr(), r.data_ptr(), 6, F.LAYOUT_ROWS, F.DTYPE_F32)
     torch.cuda.synchronize()
     t, m, h, r = t.cpu().numpy(), m.cpu().numpy(), h.float().cpu().numpy() / scale, r.cpu().numpy()
-    assert max_rel(t, want) <= 2e-6
+    # FP32 FFT rounding grows with log2(W): 12 radix-2 stages each way at W = 4096
+    assert max_rel(t, want) <= (2e-6 if nu <= 1024 else 3e-6)
     assert np.array_equal(r.transpose(0, 2, 1), t)
     assert np.array_equal(m[..., 0], t) and np.array_equal(m[..., 1], t[:, :, ::-1])
     assert max_rel(h[..., 0], want) <= 1e-3 and max_rel(h[..., 1], want[:, :, ::-1]) <= 1e-3
