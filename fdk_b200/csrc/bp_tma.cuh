@@ -80,7 +80,8 @@ constexpr unsigned kErrTimeout = 1u;
 
 struct __align__(16) TmaMeta {
     float m[12];
-    int u_lo, v_lo, staged, interior;
+    int u_lo, v_lo, staged;
+    int interior;  // every detector row v of the tile's voxels lies inside (0, nv-1): no per-slice checks
 };
 
 struct BpTmaArgs {
@@ -193,9 +194,8 @@ __device__ __forceinline__ void tile_box(const float *m, float xa, float xb, flo
     md.u_lo = u_lo;
     md.v_lo = v_lo;
     md.staged = ((int)uhi - u_lo + 1 <= C::BH && (int)vhi - v_lo + 1 <= C::BW) ? 1 : 0;
-    md.interior = (umin >= 0.f && umax < (float)(nu - 1) - 1e-3f && vmin > 1e-3f && vmax < (float)(nv - 1) - 1e-3f)
-                      ? 1
-                      : 0;
+    // u needs no tile-level flag: each column checks its own U before its slices
+    md.interior = (vmin > 1e-3f && vmax < (float)(nv - 1) - 1e-3f) ? 1 : 0;
 }
 
 // One view's contribution to a thread's column: R voxel pairs.
@@ -219,23 +219,47 @@ __device__ __forceinline__ void column_view(const TmaMeta &md, unsigned box, con
 
     if constexpr (sizeof(E) == 4) {
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
-        if (md.staged && md.interior) {
+        if (md.staged) {
             // fixed point: t = (v - v_lo) * 1024 + 1.5 * 2^23; bits = 0x4B400000 + round(1024 (v - v_lo))
             const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
             const float B1 = B * 1024.f;
             const unsigned rowp = box + (unsigned)((u0 - md.u_lo) * C::BW * 4) - (0x4B400000u >> 10) * 4u;
+            if (md.interior) {
 #pragma unroll
-            for (int k = 0; k < R; k++) {
-                const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
-                const unsigned a = rowp + (bits >> 10) * 4u;
-                const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
-                const __half2 e0 = u2h(lds32(a)), e1 = u2h(lds32(a + 4));
-                const __half2 e2 = u2h(lds32(a + C::BW * 4)), e3 = u2h(lds32(a + C::BW * 4 + 4));
-                const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
-                const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
-                const __half2 d = __hsub2(c1, c0);
-                const __half2 r = __hfma2(fvh, d, __hsub2(c0, d));
-                acc_add_f16x2(am[k], ar[k], r);
+                for (int k = 0; k < R; k++) {
+                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+                    const unsigned a = rowp + (bits >> 10) * 4u;
+                    const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
+                    const __half2 e0 = u2h(lds32(a)), e1 = u2h(lds32(a + 4));
+                    const __half2 e2 = u2h(lds32(a + C::BW * 4)), e3 = u2h(lds32(a + C::BW * 4 + 4));
+                    const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
+                    const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
+                    const __half2 d = __hsub2(c1, c0);
+                    const __half2 r = __hfma2(fvh, d, __hsub2(c0, d));
+                    acc_add_f16x2(am[k], ar[k], r);
+                }
+            } else {
+                // slices near the detector's top or bottom edge: the bounds rule of SUBPIXEL per
+                // slice (v and its mirror nv-1-v in [0, nv-1)), the same fixed-point gather inside
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const float v = fmaf(B, (float)k, A);
+                    const float vr = (float)(nv - 1) - v;
+                    const bool mv = v >= 0.f && v < (float)(nv - 1);
+                    const bool rv = vr >= 0.f && vr < (float)(nv - 1);
+                    if (!(mv || rv)) continue;
+                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+                    const unsigned a = rowp + (bits >> 10) * 4u;
+                    const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));
+                    const __half2 e0 = u2h(lds32(a)), e1 = u2h(lds32(a + 4));
+                    const __half2 e2 = u2h(lds32(a + C::BW * 4)), e3 = u2h(lds32(a + C::BW * 4 + 4));
+                    const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
+                    const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
+                    const __half2 d = __hsub2(c1, c0);
+                    const float2 rf = __half22float2(__hfma2(fvh, d, __hsub2(c0, d)));
+                    if (mv) am[k] += rf.x;
+                    if (rv) ar[k] += rf.y;
+                }
             }
             return;
         }

@@ -21,6 +21,7 @@
 // each detector column's G consecutive elements as one 16-byte store.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -73,12 +74,14 @@ __device__ __forceinline__ float row_sample(const FilterArgs &a, const float *vi
 // there.  Butterfly: (x, y) -> (x + y, (x - y) tw[(i & (half-1)) << stage]).  hb_tab (last pass
 // only) multiplies the bit-reversed result by H[bitrev(p)] / W.
 template <int NS>
-__device__ __forceinline__ void dif_pass(float2 *buf, const float2 *__restrict__ tw, const float *__restrict__ hb_tab,
-                                         int W, int log2W, int s0) {
+__device__ __forceinline__ void dif_pass(float2 *buf0, const float2 *__restrict__ tw, const float *__restrict__ hb_tab,
+                                         int W, int log2W, int s0, int count) {
     constexpr int GS = 1 << NS;
     const int hbit = log2W - 1 - s0;
     const int low = hbit - NS + 1;
-    for (int g = threadIdx.x; g < (W >> NS); g += blockDim.x) {
+    for (int gg = threadIdx.x; gg < (count << (log2W - NS)); gg += blockDim.x) {
+        float2 *buf = buf0 + ((gg >> (log2W - NS)) << log2W);  // FFT gg / (W >> NS) of count
+        const int g = gg & ((W >> NS) - 1);
         const int base = ((g >> low) << (hbit + 1)) | (g & ((1 << low) - 1));
         float2 v[GS];
 #pragma unroll
@@ -111,9 +114,12 @@ __device__ __forceinline__ void dif_pass(float2 *buf, const float2 *__restrict__
 // One pass of NS consecutive radix-2 DIT stages on index bits b0 .. b0+NS-1 (half = 2^b0 first).
 // Butterfly: t = y conj(tw[(i & (half-1)) * W / (2 half)]); (x, y) -> (x + t, x - t).
 template <int NS>
-__device__ __forceinline__ void dit_pass(float2 *buf, const float2 *__restrict__ tw, int W, int log2W, int b0) {
+__device__ __forceinline__ void dit_pass(float2 *buf0, const float2 *__restrict__ tw, int W, int log2W, int b0,
+                                         int count) {
     constexpr int GS = 1 << NS;
-    for (int g = threadIdx.x; g < (W >> NS); g += blockDim.x) {
+    for (int gg = threadIdx.x; gg < (count << (log2W - NS)); gg += blockDim.x) {
+        float2 *buf = buf0 + ((gg >> (log2W - NS)) << log2W);
+        const int g = gg & ((W >> NS) - 1);
         const int base = ((g >> b0) << (b0 + NS)) | (g & ((1 << b0) - 1));
         float2 v[GS];
 #pragma unroll
@@ -137,21 +143,22 @@ __device__ __forceinline__ void dit_pass(float2 *buf, const float2 *__restrict__
     }
 }
 
-// Forward transform, multiply by H, inverse transform of buf (W points); ends after a barrier.
-__device__ __forceinline__ void filter_fft(float2 *buf, const FilterArgs &a) {
+// Forward transform, multiply by H, inverse transform of `count` W-point FFTs stored one after
+// the other in buf; ends after a barrier.
+__device__ __forceinline__ void filter_fft(float2 *buf, const FilterArgs &a, int count = 1) {
     for (int s = 0; s < a.log2W; s += 3) {
         const int ns = min(3, a.log2W - s);
         const float *h = (s + ns == a.log2W) ? a.hb : nullptr;
-        if (ns == 3) dif_pass<3>(buf, a.tw, h, a.W, a.log2W, s);
-        else if (ns == 2) dif_pass<2>(buf, a.tw, h, a.W, a.log2W, s);
-        else dif_pass<1>(buf, a.tw, h, a.W, a.log2W, s);
+        if (ns == 3) dif_pass<3>(buf, a.tw, h, a.W, a.log2W, s, count);
+        else if (ns == 2) dif_pass<2>(buf, a.tw, h, a.W, a.log2W, s, count);
+        else dif_pass<1>(buf, a.tw, h, a.W, a.log2W, s, count);
         __syncthreads();
     }
     for (int b = 0; b < a.log2W; b += 3) {
         const int ns = min(3, a.log2W - b);
-        if (ns == 3) dit_pass<3>(buf, a.tw, a.W, a.log2W, b);
-        else if (ns == 2) dit_pass<2>(buf, a.tw, a.W, a.log2W, b);
-        else dit_pass<1>(buf, a.tw, a.W, a.log2W, b);
+        if (ns == 3) dit_pass<3>(buf, a.tw, a.W, a.log2W, b, count);
+        else if (ns == 2) dit_pass<2>(buf, a.tw, a.W, a.log2W, b, count);
+        else dit_pass<1>(buf, a.tw, a.W, a.log2W, b, count);
         __syncthreads();
     }
 }
@@ -234,29 +241,35 @@ struct PairOf<__half> {
 };
 
 // MIRROR layout, G row pairs (r, nv-1-r), r = G * blockIdx.x + g, per CTA; G * sizeof(pair) = 16.
+// NP = min(G, 4096 / W) pairs are transformed at once, so every 3-stage pass keeps all 512
+// threads busy (W / 8 groups per FFT).
 template <typename OUT, int G>
 __global__ void __launch_bounds__(512) filter_mirror_kernel(FilterArgs a) {
     using P = typename PairOf<OUT>::T;
     static_assert(G * sizeof(P) == 16, "one 16-byte store per column and side");
     extern __shared__ __align__(16) unsigned char fsm[];
-    float2 *buf = reinterpret_cast<float2 *>(fsm);
-    P *stg = reinterpret_cast<P *>(fsm + sizeof(float2) * a.W);  // [side][u][G]
-    __shared__ float pads[4];
+    const int NP = min(G, max(1, 4096 >> a.log2W));
+    float2 *buf = reinterpret_cast<float2 *>(fsm);                    // NP x W
+    P *stg = reinterpret_cast<P *>(fsm + sizeof(float2) * NP * a.W);  // [side][u][G]
+    __shared__ float pads[4 * G];
     const int view = blockIdx.y, r0 = blockIdx.x * G;
     const float *vsrc = a.src + (long long)view * a.src_vstride;
-    for (int g = 0; g < G; g++) {
-        const int r1 = r0 + g, r2 = a.nv - 1 - r1;
-        if (threadIdx.x < 4) pads[threadIdx.x] = edge_mean(a, vsrc, threadIdx.x < 2 ? r1 : r2, (threadIdx.x & 1) == 0);
-        __syncthreads();  // also ends the previous pair's reads of buf
-        for (int k = threadIdx.x; k < a.W; k += blockDim.x) {
-            const int c = k - a.off;
+    for (int g0 = 0; g0 < G; g0 += NP) {
+        if (threadIdx.x < 4 * NP) {
+            const int q = threadIdx.x >> 2, j = threadIdx.x & 3, r1 = r0 + g0 + q;
+            pads[threadIdx.x] = edge_mean(a, vsrc, j < 2 ? r1 : a.nv - 1 - r1, (j & 1) == 0);
+        }
+        __syncthreads();  // also ends the previous pairs' reads of buf
+        for (int k = threadIdx.x; k < (NP << a.log2W); k += blockDim.x) {
+            const int q = k >> a.log2W, c = (k & (a.W - 1)) - a.off;
+            const int r1 = r0 + g0 + q, r2 = a.nv - 1 - r1;
             float x1, x2;
             if (c < 0) {
-                x1 = pads[0];
-                x2 = pads[2];
+                x1 = pads[4 * q];
+                x2 = pads[4 * q + 2];
             } else if (c >= a.nu) {
-                x1 = pads[1];
-                x2 = pads[3];
+                x1 = pads[4 * q + 1];
+                x2 = pads[4 * q + 3];
             } else {
                 x1 = row_sample(a, vsrc, r1, c);
                 x2 = row_sample(a, vsrc, r2, c);
@@ -264,9 +277,10 @@ __global__ void __launch_bounds__(512) filter_mirror_kernel(FilterArgs a) {
             buf[k] = make_float2(x1, x2);
         }
         __syncthreads();
-        filter_fft(buf, a);
-        for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
-            const float2 y = buf[a.off + u];
+        filter_fft(buf, a, NP);
+        for (int k = threadIdx.x; k < NP * a.nu; k += blockDim.x) {
+            const int q = k / a.nu, u = k - q * a.nu, g = g0 + q;
+            const float2 y = buf[(q << a.log2W) + a.off + u];
             const OUT o1 = to_out<OUT>(a, y.x), o2 = to_out<OUT>(a, y.y);
             stg[u * G + g] = PairOf<OUT>::make(o1, o2);                     // element (u, r1)
             stg[(a.nu + u) * G + (G - 1 - g)] = PairOf<OUT>::make(o2, o1);  // element (u, r2)
@@ -315,7 +329,8 @@ void FilterTables::release() {
 template <typename OUT, int G>
 static int launch_mirror(const FilterArgs &a, int n_views, cudaStream_t st) {
     using P = typename PairOf<OUT>::T;
-    const size_t smem = sizeof(float2) * a.W + 2 * sizeof(P) * G * a.nu;
+    const int np = std::min(G, std::max(1, 4096 >> a.log2W));
+    const size_t smem = sizeof(float2) * np * a.W + 2 * sizeof(P) * G * a.nu;
     if (smem > 48 * 1024)  // per device and size: cheap, so set on every launch
         FDK_CUDA(cudaFuncSetAttribute(filter_mirror_kernel<OUT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
@@ -329,7 +344,7 @@ static int launch_filter(const FilterArgs &a, int n_views, int layout, int dtype
         // grouped kernel when G pairs tile the rows and every 16-byte store is aligned
         const int G = dtype == FDK_DTYPE_F32 ? 2 : 4;
         const size_t pair = dtype == FDK_DTYPE_F32 ? 8 : 4;
-        const size_t smem = sizeof(float2) * a.W + 2 * pair * G * a.nu;
+        const size_t smem = sizeof(float2) * std::max(a.W, std::min(G, 4096 / a.W) * a.W) + 2 * pair * G * a.nu;
         if (a.nv % (2 * G) == 0 && ((uintptr_t)a.dst & 15) == 0 && (a.dst_pitch * pair) % 16 == 0 &&
             (a.dst_vstride * (pair / 2)) % 16 == 0 && smem <= 200 * 1024) {
             if (dtype == FDK_DTYPE_F32) return launch_mirror<float, 2>(a, n_views, st);

@@ -41,6 +41,9 @@ struct fdk_recon {
     cudaEvent_t raw_ready[2] = {nullptr, nullptr}, raw_free[2] = {nullptr, nullptr};
     cudaEvent_t f0 = nullptr, f1 = nullptr, done = nullptr;
     int slot = 0;
+    // filtered views waiting in d_filt for a full batch: views pend_first .. pend_first+pending-1
+    int pending = 0;
+    long long pend_first = 0;
     double filter_ms = 0;
     long long views = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
@@ -100,23 +103,43 @@ int collect_filter_timers(fdk_recon *h) {
 }
 
 // Filter + backproject views [first, first+n) whose raw data is at d_src (nv x nu each).
+// Backproject the filtered views waiting in d_filt (one launch), on the compute stream.
+int flush_pending(fdk_recon *h) {
+    if (h->pending == 0) return FDK_OK;
+    FDK_TRY(fdk_bp_bp_device_mats_internal(h->bp, h->d_filt, h->layout, h->d_mats + 12 * h->pend_first, h->pending,
+                                           h->mats.data() + 12 * h->pend_first, h->compute));
+    h->pending = 0;
+    return FDK_OK;
+}
+
+// Filter n raw views (device) into the batch buffer behind the views already waiting there;
+// a full batch is backprojected at once.  Views join a batch only when they continue it
+// (first == pend_first + pending); otherwise the waiting views are backprojected first.
 int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cudaEvent_t release) {
     const fdk_geometry &g = h->g;
     const long long frame = g.nu * g.nv;
+    const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
+    const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
+    if (h->pending > 0 && first != h->pend_first + h->pending) FDK_TRY(flush_pending(h));
     std::pair<cudaEvent_t, cudaEvent_t> t;
     FDK_CUDA(cudaEventCreate(&t.first));
     FDK_CUDA(cudaEventCreate(&t.second));
     FDK_CUDA(cudaEventRecord(t.first, h->compute));
-    const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
-    FDK_TRY(filter_views(d_src, (int)g.nu, frame, h->d_filt, (int)g.nv, dstride, h->d_cos, (int)g.nu, h->tables,
-                         (int)g.nu, (int)g.nv, h->pad, n, h->layout, h->dtype,
-                         h->compute, h->out_scale, h->d_overflow));
+    for (int done = 0; done < n;) {
+        if (h->pending == 0) h->pend_first = first + done;
+        const int m = std::min(n - done, h->batch - h->pending);
+        void *dst = static_cast<unsigned char *>(h->d_filt) + (size_t)h->pending * dstride * esz;
+        FDK_TRY(filter_views(d_src + (long long)done * frame, (int)g.nu, frame, dst, (int)g.nv, dstride, h->d_cos,
+                             (int)g.nu, h->tables, (int)g.nu, (int)g.nv, h->pad, m, h->layout, h->dtype, h->compute,
+                             h->out_scale, h->d_overflow));
+        h->pending += m;
+        done += m;
+        if (h->pending == h->batch) FDK_TRY(flush_pending(h));
+    }
     FDK_CUDA(cudaEventRecord(t.second, h->compute));
     h->ftimers.push_back(t);
     if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
     if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
-    FDK_TRY(fdk_bp_bp_device_mats_internal(h->bp, h->d_filt, h->layout, h->d_mats + 12 * first, n,
-                                           h->mats.data() + 12 * first, h->compute));
     h->views += n;
     return FDK_OK;
 }
@@ -318,11 +341,21 @@ int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, i
     FDK_ABI_END
 }
 
+int fdk_recon_flush(fdk_recon *h) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    return flush_pending(h);
+    FDK_ABI_END
+}
+
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
+    FDK_TRY(flush_pending(h));
     FDK_CUDA(cudaEventRecord(h->done, h->compute));
     const auto t0 = std::chrono::steady_clock::now();
     const int64_t limit = timeout_ms > 0 ? timeout_ms : 600000;
@@ -379,6 +412,7 @@ int fdk_recon_reset(fdk_recon *h) {
     FDK_CUDA(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)));
     h->filter_ms = 0;
     h->views = 0;
+    h->pending = 0;  // filtered views not yet backprojected are dropped with the volume
     return fdk_bp_reset(h->bp);
     FDK_ABI_END
 }

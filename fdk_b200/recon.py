@@ -44,6 +44,10 @@ class Reconstructor:
     def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push(self._h, host_ptr, first, n))
 
+    def flush(self) -> None:
+        """Backproject the filtered views waiting for a full batch now (asynchronous)."""
+        check(lib().fdk_recon_flush(self._h))
+
     def push_folder(self, folder: str, first: int, n: int, step: int = 1, start: int = 0, threads: int = 0) -> None:
         """Views first..first+n-1 from a projection folder (img%04d.raw, view v in file v*step+start),
         read into pinned staging while the previous batch is copied and reconstructed."""

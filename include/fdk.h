@@ -218,7 +218,8 @@ int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_s
 typedef struct fdk_recon fdk_recon;
 /* A reconstructor for geometry g: cosine weight + ramp filter + backprojection of the whole
  * volume (mirror slab pair, as DivVolume with one rank, cuFDK/mpiFDK.h:116-149).
- * batch: views per internal batch (multiple of 2, <= 128).  precision: FDK_BP_*. */
+ * batch: views per backprojection launch (<= 128; <= 32 for FDK_BP_FP32_EXACT), independent of
+ * how many views each push carries.  precision: FDK_BP_*. */
 int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch,
                      int32_t device);
 /* The same for one mirror-symmetric slab pair of the volume (one rank of DivVolume,
@@ -241,6 +242,10 @@ int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, i
  * batch k.  Every file's size is checked before any is read (FDK_ERR_IO names the first bad one). */
 int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64_t n, int32_t step,
                           int32_t start, int32_t threads);
+/* Pushed views are filtered at once and backprojected a full batch at a time (views that do not
+ * continue the waiting batch close it first).  fdk_recon_flush launches the backprojection of a
+ * partial batch now (asynchronous); fdk_recon_sync and fdk_recon_get_volume flush implicitly. */
+int fdk_recon_flush(fdk_recon *h);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
 /* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).

@@ -143,6 +143,7 @@ class Reconstructor {
                     int threads = 0) {
         check(fdk_recon_push_folder(h_, folder.c_str(), first, n, step, start, threads));
     }
+    void Flush() { check(fdk_recon_flush(h_)); }
     void Sync(int64_t timeout_ms = 0) { check(fdk_recon_sync(h_, timeout_ms)); }
     void GetVolume(float *host_vol, int64_t size) { check(fdk_recon_get_volume(h_, host_vol, size)); }
     fdk_recon *handle() { return h_; }

@@ -47,8 +47,9 @@ def test_reconstructor_vs_oracle(precision):
     if precision == "mixed":
         assert e64 <= 1e-3
     else:
-        # the batches as pushed: 16 + 9 views, then 15 (each backprojection launch adds its sum)
-        bs = [(filt[0:16], mats[0:16]), (filt[16:25], mats[16:25]), (filt[25:40], mats[25:40])]
+        # backprojection launches: full batches of 16 across the two pushes (25 + 15 views), then
+        # the remaining 8 at sync; each launch adds its sum to the volume
+        bs = [(filt[0:16], mats[0:16]), (filt[16:32], mats[16:32]), (filt[32:40], mats[32:40])]
         ref32 = oracle_bp_ref32(top, bot[5], n, [b[0] for b in bs], [b[1] for b in bs])
         e32 = rel_l2(got[m], ref32[m])
         print(precision, "rel-L2 vs reference arithmetic", e32)
@@ -151,3 +152,22 @@ def test_push_folder_matches_push(tmp_path):
     b.push_folder(str(tmp_path), 0, 10, step=2, threads=3)
     b.push_folder(str(tmp_path), 10, views - 10, step=2)
     np.testing.assert_array_equal(a.volume(), b.volume())
+
+
+def test_batching_is_independent_of_push_pattern():
+    """Pushes of any size and order fill the backprojection batches the same way up to FP32
+    summation order: out-of-order pushes close the waiting batch, flush() launches a partial one."""
+    n, views = 32, 40
+    p = small_param(n, 48, 40, views)
+    _, proj = phantom_views(p, seed=4)
+    a = F.Reconstructor(p, "fp32", batch=16)
+    a.push(proj.copy(), 0)
+    b = F.Reconstructor(p, "fp32", batch=16)
+    b.push(proj[20:30].copy(), 20)
+    b.push(proj[0:7].copy(), 0)
+    b.flush()
+    b.push(proj[7:20].copy(), 7)
+    b.push(proj[30:].copy(), 30)
+    va, vb = a.volume(), b.volume()
+    assert b.stats()["views"] == views
+    assert rel_l2(vb, va) <= 1e-6
