@@ -49,6 +49,8 @@ EXPORTED = [
     "fdk_voxelize", "fdk_rows_to_mirror", "fdk_volume_mse", "fdk_bp_adjoint",
     "fdk_proj_path", "fdk_load_proj_folder", "fdk_save_proj_folder", "fdk_save_volume", "fdk_load_volume",
     "fdk_save_volume_slices",
+    "fdk_toeplitz_create", "fdk_toeplitz_run_device", "fdk_toeplitz_check", "fdk_toeplitz_matrix",
+    "fdk_toeplitz_destroy",
 ]
 
 
@@ -157,6 +159,11 @@ def lib() -> C.CDLL:
         "fdk_save_volume": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
         "fdk_load_volume": ([C.c_char_p, vp, i64, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
         "fdk_save_volume_slices": ([C.c_char_p, vp, i32, i32, i32, i32, i32], C.c_int),
+        "fdk_toeplitz_create": ([C.POINTER(vp), vp, vp, i64, i64, i64, i32, i32, C.c_float, i32], C.c_int),
+        "fdk_toeplitz_run_device": ([vp, vp, vp, i64, i32, C.c_float, vp], C.c_int),
+        "fdk_toeplitz_check": ([vp], C.c_int),
+        "fdk_toeplitz_matrix": ([vp, i64, i64, i32, vp], C.c_int),
+        "fdk_toeplitz_destroy": ([vp], C.c_int),
         "fdk_probe_smem": ([i32, f64p], C.c_int),
         "fdk_probe_fma": ([i32, f64p], C.c_int),
     }

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfdk_b200.so")
 SOURCES = ["geometry.cpp", "filter.cu", "filter_noalloc.cu", "bp.cu", "rtk.cu", "phantom.cu", "recon.cu",
-           "probe.cu", "fproj.cu", "learn.cu", "io.cpp"]
+           "probe.cu", "fproj.cu", "learn.cu", "io.cpp", "toeplitz.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -4,6 +4,7 @@
   ``FilterEngine(cos_image_table, fft_kernel_real_f32).Filtering(src, dst, transpose)``.
 * ``filter_row_real32`` / ``correct_image_real32`` mirror the cuFFT plugin
   (FilterlibCufft/cudaFftFilter.cuh:6-8) on device buffers.
+* ``ToeplitzFilter`` is the same filter as a tensor-core GEMM (no reference counterpart).
 """
 from __future__ import annotations
 
@@ -83,3 +84,44 @@ def filter_row_real32(src, dst, filt) -> None:
 
 __all__ = ["FilterEngine", "correct_image_real32", "filter_row_real32", "LAYOUT_ROWS", "LAYOUT_TRANSPOSED",
            "LAYOUT_MIRROR", "DTYPE_F32", "DTYPE_F16"]
+
+
+class ToeplitzFilter:
+    """The row filter as a GEMM on the tensor cores (fdk_toeplitz_*): y = M (in_scale * cos * p)
+    per row, M the nu x nu matrix of the fused filter, FP16 or BF16 operands, FP32 accumulation,
+    FP16 output (ROWS or MIRROR layout).  No reference counterpart."""
+
+    def __init__(self, cos_table: np.ndarray, H: np.ndarray, pad_edge: int = 4, dtype: str = "f16",
+                 in_scale: float = 1.0, device: int = 0):
+        cos = np.ascontiguousarray(cos_table, np.float32)
+        self.nv, self.nu = cos.shape
+        h = np.ascontiguousarray(H, np.float64)
+        self._h = C.c_void_p()
+        check(lib().fdk_toeplitz_create(C.byref(self._h), cos.ctypes.data, h.ctypes.data, self.nu, self.nv, h.size,
+                                        pad_edge, 1 if dtype == "bf16" else 0, in_scale, device))
+
+    def run_device(self, src_ptr: int, dst_ptr: int, n_views: int, layout: int = LAYOUT_ROWS, out_scale: float = 1.0,
+                   stream: int = 0) -> None:
+        check(lib().fdk_toeplitz_run_device(self._h, src_ptr, dst_ptr, n_views, layout, out_scale, stream))
+
+    def check(self) -> None:
+        check(lib().fdk_toeplitz_check(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            lib().fdk_toeplitz_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def toeplitz_matrix(H: np.ndarray, nu: int, pad_edge: int = 4) -> np.ndarray:
+    """FP64 filter matrix M (nu x nu) of the fused filter with response H (W taps)."""
+    h = np.ascontiguousarray(H, np.float64)
+    out = np.empty((nu, nu), np.float64)
+    check(lib().fdk_toeplitz_matrix(h.ctypes.data, h.size, nu, pad_edge, out.ctypes.data))
+    return out

@@ -131,6 +131,24 @@ int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, in
                           int32_t layout, int32_t out_dtype, float out_scale, void *stream);
 int fdk_filter_destroy(fdk_filter *h);
 
+/* The same filter as a GEMM on the tensor cores (no reference counterpart; the north star's
+ * "Toeplitz row-GEMM ... BF16 in, FP32 accumulate").  Per row, y = M (in_scale * cos * p) with M
+ * the nu x nu matrix of the fused filter (edge-mean pads, circular kernel IDFT(H), crop; built in
+ * FP64, stored FP16 or BF16 when bf16 != 0).  nu must be a multiple of 256, nv of 128, and the
+ * device an sm_100 GPU (FDK_ERR_UNSUPPORTED otherwise). */
+typedef struct fdk_toeplitz fdk_toeplitz;
+int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double *H, int64_t nu, int64_t nv,
+                        int64_t W, int32_t pad_edge, int32_t bf16, float in_scale, int32_t device);
+/* n_views raw FP32 views (nv x nu each, device) -> FP16 output * out_scale, ROWS or MIRROR
+ * layout, asynchronous on stream. */
+int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst, int64_t n_views, int32_t layout,
+                            float out_scale, void *stream);
+/* After a sync: FDK_ERR_DEVICE_CHECK if a pipeline wait timed out or an output left the FP16 range. */
+int fdk_toeplitz_check(fdk_toeplitz *h);
+/* The FP64 filter matrix M (nu x nu, row-major, out[u * nu + c]) of filter response H (W taps). */
+int fdk_toeplitz_matrix(const double *H, int64_t W, int64_t nu, int32_t pad_edge, double *out);
+int fdk_toeplitz_destroy(fdk_toeplitz *h);
+
 /* FilterlibCufft plugin (FilterlibCufft/cudaFftFilter.cuh:6-8, cudaFftFilter.cu:283-392).
  * DataRef<float> (FilterlibCufft/cudaBackProjection.cuh:121-230) as a plain struct: device data,
  * width (fast axis), height, depth, pitch in elements.

@@ -1,0 +1,34 @@
+"""Tensor-core filter (tcgen05 GEMM, FP16/BF16 operands, FP32 accumulation) against the FP64
+oracle filter, in both output layouts."""
+import numpy as np
+import pytest
+
+import fdk_b200 as F
+from tests.helpers import oracle_filtered, phantom_views, rel_l2, small_param
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("nu,nv,views,dtype", [(256, 128, 3, "f16"), (512, 256, 2, "f16"), (1536, 128, 1, "f16"),
+                                               (512, 128, 2, "bf16")])
+def test_toeplitz_gemm_vs_oracle(nu, nv, views, dtype):
+    import torch
+
+    p = small_param(64, nu, nv, views)
+    _, proj = phantom_views(p)
+    s = float(1.0 / (p.SOD * p.SOD * p.AngularAndrampFactor))  # line-integral units
+    tf = F.ToeplitzFilter(p.cos_sigma, p.fft_kernel_real, 4, dtype, in_scale=s)
+    src = torch.from_numpy(np.ascontiguousarray(proj, np.float32)).cuda()
+    rows = torch.empty((views, nv, nu), dtype=torch.float16, device="cuda")
+    tf.run_device(src.data_ptr(), rows.data_ptr(), views, F.LAYOUT_ROWS, 1.0)
+    mir = torch.empty((views, nu, nv, 2), dtype=torch.float16, device="cuda")
+    tf.run_device(src.data_ptr(), mir.data_ptr(), views, F.LAYOUT_MIRROR, 1.0)
+    torch.cuda.synchronize()
+    tf.check()
+    want = oracle_filtered(p, proj) * s  # (views, nu, nv)
+    got = rows.float().cpu().numpy().transpose(0, 2, 1)
+    e = rel_l2(got, want)
+    print(dtype, nu, nv, "rel-L2 vs FP64", e, "max", np.abs(got - want).max() / np.abs(want).max())
+    assert e <= (2e-3 if dtype == "f16" else 1.5e-2), e
+    m = mir.float().cpu().numpy()
+    assert np.array_equal(m[..., 0], got) and np.array_equal(m[..., 1], got[:, :, ::-1])
