@@ -387,6 +387,7 @@ struct fdk_toeplitz {
     int nu = 0, nv = 0, W = 0, pad = 4;
     bool bf16 = false;
     float in_scale = 1.f;
+    float m_unscale = 1.f;      // M is stored times 2^e (FP16 normal range); outputs times 2^-e
     float *d_cos = nullptr;
     void *d_M = nullptr;        // nu x nu, 16-bit
     void *d_x = nullptr;        // views x nv x nu, 16-bit (weighted input)
@@ -425,13 +426,22 @@ int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double
     h->in_scale = in_scale;
     std::vector<double> M;
     toeplitz_matrix(H, (int)W, (int)nu, pad_edge, M);
+    // FP16: scale M by a power of two so its largest entry sits near 2^14; the kernel's small
+    // far-off-diagonal taps (the ramp's low-frequency response) then stay out of the subnormal
+    // range.  The output scale divides the same power out exactly.
+    double mmax = 0;
+    for (double x : M) mmax = std::max(mmax, std::fabs(x));
+    int e = 0;
+    if (!h->bf16 && mmax > 0) e = 14 - (int)std::ceil(std::log2(mmax));
+    h->m_unscale = (float)std::ldexp(1.0, -e);
     std::vector<unsigned short> m16((size_t)nu * nu);
     for (size_t i = 0; i < m16.size(); i++) {
+        const float x = (float)std::ldexp(M[i], e);
         if (h->bf16) {
-            const __nv_bfloat16 b = __float2bfloat16_rn((float)M[i]);
+            const __nv_bfloat16 b = __float2bfloat16_rn(x);
             m16[i] = *reinterpret_cast<const unsigned short *>(&b);
         } else {
-            const __half b = __float2half_rn((float)M[i]);
+            const __half b = __float2half_rn(x);
             m16[i] = *reinterpret_cast<const unsigned short *>(&b);
         }
     }
@@ -506,7 +516,7 @@ int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst
     g.R = (int)R;
     g.N = h->nu;
     g.K = h->nu;
-    g.out_scale = out_scale;
+    g.out_scale = out_scale * h->m_unscale;
     g.err = h->d_err;
     g.overflow = h->d_err + 1;
     const long long tiles = (R / tpz::BM) * (h->nu / tpz::BN);
