@@ -159,7 +159,7 @@ def lib() -> C.CDLL:
         "fdk_save_volume": ([C.c_char_p, vp, i32, i32, i32], C.c_int),
         "fdk_load_volume": ([C.c_char_p, vp, i64, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)], C.c_int),
         "fdk_save_volume_slices": ([C.c_char_p, vp, i32, i32, i32, i32, i32], C.c_int),
-        "fdk_toeplitz_create": ([C.POINTER(vp), vp, vp, i64, i64, i64, i32, i32, C.c_float, i32], C.c_int),
+        "fdk_toeplitz_create": ([C.POINTER(vp), vp, vp, i64, i64, i64, i32, i32, i32, C.c_float, i32], C.c_int),
         "fdk_toeplitz_run_device": ([vp, vp, vp, i64, i32, C.c_float, vp], C.c_int),
         "fdk_toeplitz_check": ([vp], C.c_int),
         "fdk_toeplitz_matrix": ([vp, i64, i64, i32, vp], C.c_int),

@@ -10,7 +10,10 @@
 // FilterLib.h:26-46 and cudaFftFilter.cu kernelPad).  M is built once in FP64 on the host and
 // stored FP16 or BF16; a batch of views is then one GEMM  Y[R][nu] = X[R][nu] . M^T  with R =
 // views x nv rows, FP16/BF16 operands and FP32 accumulation (north star: "a Toeplitz row-GEMM on
-// the tensor cores (BF16 in, FP32 accumulate)").
+// the tensor cores (BF16 in, FP32 accumulate)").  The ramp filter cancels most of its input, so
+// 16-bit input rounding shows up ~10x larger in its output; the split mode keeps the operands'
+// low parts too, x = x_hi + x_lo and M = M_hi + M_lo, and sums x_hi M_hi + x_lo M_hi + x_hi M_lo
+// in the same GEMM with K = 3 nu (three times the FLOPs, close to FP32 accuracy).
 //
 // GEMM kernel (sm_100a, one CTA per SM, persistent over 128 x 256 output tiles):
 //   warp 0  TMA producer: A (128 rows x 64 K) and B (256 rows x 64 K) boxes with 128-byte
@@ -281,16 +284,31 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_gemm_kernel(const __grid_
     if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
-// x16[r][c] = (p[r][c] * cos[r % nv][c] * in_scale) as FP16/BF16, R rows of nu
+template <typename T>
+__device__ __forceinline__ T to16(float x) {
+    if constexpr (std::is_same<T, __half>::value) return __float2half_rn(x);
+    else return __float2bfloat16_rn(x);
+}
+template <typename T>
+__device__ __forceinline__ float from16(T x) {
+    if constexpr (std::is_same<T, __half>::value) return __half2float(x);
+    else return __bfloat162float(x);
+}
+
+// A operand rows: x = p * cos * in_scale (R rows of nu) as T segments of nu values each:
+// terms 1: [hi]; 2: [hi | lo]; 3: [hi | lo | hi], hi = round16(x), lo = round16(x - hi)
 template <typename T>
 __global__ void weight_convert_kernel(const float *__restrict__ src, const float *__restrict__ cos, T *__restrict__ dst,
-                                      long long n, int nu, int nv, float in_scale) {
+                                      long long n, int nu, int nv, float in_scale, int terms) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const long long row = i / nu;
         const int c = (int)(i - row * nu), v = (int)(row % nv);
         const float x = src[i] * (cos ? cos[(long long)v * nu + c] : 1.f) * in_scale;
-        if constexpr (std::is_same<T, __half>::value) dst[i] = __float2half_rn(x);
-        else dst[i] = __float2bfloat16_rn(x);
+        const T hi = to16<T>(x);
+        T *d = dst + row * (long long)nu * terms + c;
+        d[0] = hi;
+        if (terms > 1) d[nu] = to16<T>(x - from16<T>(hi));
+        if (terms > 2) d[2 * nu] = hi;
     }
 }
 
@@ -386,6 +404,7 @@ struct fdk_toeplitz {
     int device = 0;
     int nu = 0, nv = 0, W = 0, pad = 4;
     bool bf16 = false;
+    int terms = 1;              // 1 plain; 3: (x_hi, x_lo, x_hi) . (M_hi, M_hi, M_lo)
     float in_scale = 1.f;
     float m_unscale = 1.f;      // M is stored times 2^e (FP16 normal range); outputs times 2^-e
     float *d_cos = nullptr;
@@ -400,7 +419,7 @@ struct fdk_toeplitz {
 extern "C" {
 
 int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double *H, int64_t nu, int64_t nv,
-                        int64_t W, int32_t pad_edge, int32_t bf16, float in_scale, int32_t device) {
+                        int64_t W, int32_t pad_edge, int32_t bf16, int32_t split, float in_scale, int32_t device) {
     FDK_ABI_BEGIN
     clear_error();
     FDK_CHECK_ARG(out && H, "NULL argument");
@@ -423,6 +442,7 @@ int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double
     h->W = (int)W;
     h->pad = pad_edge;
     h->bf16 = bf16 != 0;
+    h->terms = split ? 3 : 1;
     h->in_scale = in_scale;
     std::vector<double> M;
     toeplitz_matrix(H, (int)W, (int)nu, pad_edge, M);
@@ -434,17 +454,31 @@ int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double
     int e = 0;
     if (!h->bf16 && mmax > 0) e = 14 - (int)std::ceil(std::log2(mmax));
     h->m_unscale = (float)std::ldexp(1.0, -e);
-    std::vector<unsigned short> m16((size_t)nu * nu);
-    for (size_t i = 0; i < m16.size(); i++) {
-        const float x = (float)std::ldexp(M[i], e);
+    // B rows: [M_hi] or [M_hi | M_hi | M_lo] (K = terms * nu)
+    const int T = h->terms;
+    std::vector<unsigned short> m16((size_t)nu * nu * T);
+    auto enc16 = [&](double x, double *back) -> unsigned short {
         if (h->bf16) {
-            const __nv_bfloat16 b = __float2bfloat16_rn(x);
-            m16[i] = *reinterpret_cast<const unsigned short *>(&b);
-        } else {
-            const __half b = __float2half_rn(x);
-            m16[i] = *reinterpret_cast<const unsigned short *>(&b);
+            const __nv_bfloat16 b = __float2bfloat16_rn((float)x);
+            *back = (double)__bfloat162float(b);
+            return *reinterpret_cast<const unsigned short *>(&b);
         }
-    }
+        const __half b = __float2half_rn((float)x);
+        *back = (double)__half2float(b);
+        return *reinterpret_cast<const unsigned short *>(&b);
+    };
+    for (long long u = 0; u < nu; u++)
+        for (long long c = 0; c < nu; c++) {
+            const double x = std::ldexp(M[(size_t)u * nu + c], e);
+            double hi = 0, lo = 0;
+            const unsigned short hb = enc16(x, &hi);
+            unsigned short *row = &m16[(size_t)u * nu * T];
+            row[c] = hb;
+            if (T == 3) {
+                row[nu + c] = hb;
+                row[2 * nu + c] = enc16(x - hi, &lo);
+            }
+        }
     int s = FDK_OK;
     auto step = [&](cudaError_t e, const char *what) {
         if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
@@ -493,29 +527,30 @@ int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst
         h->d_x = nullptr;
         h->d_y = nullptr;
         h->cap_views = 0;
-        FDK_CUDA(cudaMalloc(&h->d_x, 2 * frame * n_views));
+        FDK_CUDA(cudaMalloc(&h->d_x, 2 * frame * n_views * h->terms));
         FDK_CUDA(cudaMalloc((void **)&h->d_y, 2 * frame * n_views));
         h->cap_views = n_views;
     }
     const long long n = frame * n_views;
     if (h->bf16)
         tpz::weight_convert_kernel<__nv_bfloat16><<<148 * 16, 256, 0, st>>>(
-            dev_src, h->d_cos, (__nv_bfloat16 *)h->d_x, n, h->nu, h->nv, h->in_scale);
+            dev_src, h->d_cos, (__nv_bfloat16 *)h->d_x, n, h->nu, h->nv, h->in_scale, h->terms);
     else
         tpz::weight_convert_kernel<__half><<<148 * 16, 256, 0, st>>>(dev_src, h->d_cos, (__half *)h->d_x, n, h->nu,
-                                                                     h->nv, h->in_scale);
+                                                                     h->nv, h->in_scale, h->terms);
     FDK_CUDA(cudaGetLastError());
     const long long R = (long long)h->nv * n_views;
     FDK_CHECK_ARG(R < (1ll << 31), "too many rows");
     CUtensorMap ma, mb;
-    FDK_TRY(encode_2d(&ma, h->d_x, R, h->nu, tpz::BM, h->bf16));
-    FDK_TRY(encode_2d(&mb, h->d_M, h->nu, h->nu, tpz::BN, h->bf16));
+    const long long K = (long long)h->nu * h->terms;
+    FDK_TRY(encode_2d(&ma, h->d_x, R, K, tpz::BM, h->bf16));
+    FDK_TRY(encode_2d(&mb, h->d_M, h->nu, K, tpz::BN, h->bf16));
     tpz::GemmArgs g;
     __half *gout = layout == FDK_LAYOUT_ROWS ? (__half *)dev_dst : h->d_y;
     g.out = gout;
     g.R = (int)R;
     g.N = h->nu;
-    g.K = h->nu;
+    g.K = (int)K;
     g.out_scale = out_scale * h->m_unscale;
     g.err = h->d_err;
     g.overflow = h->d_err + 1;

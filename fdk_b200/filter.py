@@ -92,13 +92,13 @@ class ToeplitzFilter:
     FP16 output (ROWS or MIRROR layout).  No reference counterpart."""
 
     def __init__(self, cos_table: np.ndarray, H: np.ndarray, pad_edge: int = 4, dtype: str = "f16",
-                 in_scale: float = 1.0, device: int = 0):
+                 in_scale: float = 1.0, device: int = 0, split: bool = False):
         cos = np.ascontiguousarray(cos_table, np.float32)
         self.nv, self.nu = cos.shape
         h = np.ascontiguousarray(H, np.float64)
         self._h = C.c_void_p()
         check(lib().fdk_toeplitz_create(C.byref(self._h), cos.ctypes.data, h.ctypes.data, self.nu, self.nv, h.size,
-                                        pad_edge, 1 if dtype == "bf16" else 0, in_scale, device))
+                                        pad_edge, 1 if dtype == "bf16" else 0, 1 if split else 0, in_scale, device))
 
     def run_device(self, src_ptr: int, dst_ptr: int, n_views: int, layout: int = LAYOUT_ROWS, out_scale: float = 1.0,
                    stream: int = 0) -> None:

@@ -1,5 +1,6 @@
 """Filter variant sweep (the C4 workload by default: 1024 views of 1536 x 1024, W = 2048): the
-batched FFT filter against the tensor-core Toeplitz GEMM with FP16 and BF16 operands.  Reports
+batched FFT filter against the tensor-core Toeplitz GEMM with FP16 and BF16 operands, plain and
+split (hi + lo parts, three products).  Reports
 per variant the time per batch of views (CUDA events, inputs resident in HBM), HBM GB/s of the
 algorithmic bytes, GEMM TFLOP/s, and rel-L2 / max error of the filtered rows against the FP64
 oracle on the first view.  One JSON line.
@@ -58,11 +59,13 @@ def main():
     hbm = batch * frame * (4 + 4)
     res["variants"]["fft"] = {"ms": ms, "hbm_gbs": hbm / (ms * 1e-3) / 1e9, **errors(out)}
     flops = 2.0 * batch * nv * nu * nu
-    for dt in ("f16", "bf16"):
-        tf = F.ToeplitzFilter(p.cos_sigma, p.fft_kernel_real, 4, dt, in_scale=s)
+    for dt, split in (("f16", False), ("bf16", False), ("f16", True), ("bf16", True)):
+        tf = F.ToeplitzFilter(p.cos_sigma, p.fft_kernel_real, 4, dt, in_scale=s, split=split)
         ms = timed(lambda: tf.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, 1.0))
         tf.check()
-        res["variants"][f"toeplitz_{dt}"] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, **errors(out)}
+        terms = 3 if split else 1
+        res["variants"][f"toeplitz_{dt}{'_split' if split else ''}"] = {
+            "ms": ms, "tflops": terms * flops / (ms * 1e-3) / 1e12, **errors(out)}
         tf.close()
     print(json.dumps(res), flush=True)
 

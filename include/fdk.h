@@ -134,11 +134,12 @@ int fdk_filter_destroy(fdk_filter *h);
 /* The same filter as a GEMM on the tensor cores (no reference counterpart; the north star's
  * "Toeplitz row-GEMM ... BF16 in, FP32 accumulate").  Per row, y = M (in_scale * cos * p) with M
  * the nu x nu matrix of the fused filter (edge-mean pads, circular kernel IDFT(H), crop; built in
- * FP64, stored FP16 or BF16 when bf16 != 0).  nu must be a multiple of 256, nv of 128, and the
- * device an sm_100 GPU (FDK_ERR_UNSUPPORTED otherwise). */
+ * FP64, stored FP16 or BF16 when bf16 != 0).  split != 0 keeps the low parts of both operands
+ * (x_hi M_hi + x_lo M_hi + x_hi M_lo, three times the FLOPs, close to FP32 accuracy).  nu must be
+ * a multiple of 256, nv of 128, and the device an sm_100 GPU (FDK_ERR_UNSUPPORTED otherwise). */
 typedef struct fdk_toeplitz fdk_toeplitz;
 int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double *H, int64_t nu, int64_t nv,
-                        int64_t W, int32_t pad_edge, int32_t bf16, float in_scale, int32_t device);
+                        int64_t W, int32_t pad_edge, int32_t bf16, int32_t split, float in_scale, int32_t device);
 /* n_views raw FP32 views (nv x nu each, device) -> FP16 output * out_scale, ROWS or MIRROR
  * layout, asynchronous on stream. */
 int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst, int64_t n_views, int32_t layout,
