@@ -44,6 +44,13 @@ class Reconstructor:
     def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push(self._h, host_ptr, first, n))
 
+    @property
+    def filter_kind(self) -> str:
+        """'fft' or 'tensor' (the split-FP16 tcgen05 GEMM filter)."""
+        k = C.c_int32()
+        check(lib().fdk_recon_filter_kind(self._h, C.byref(k)))
+        return "tensor" if k.value == 1 else "fft"
+
     def flush(self) -> None:
         """Backproject the filtered views waiting for a full batch now (asynchronous)."""
         check(lib().fdk_recon_flush(self._h))

@@ -265,6 +265,10 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
  * continue the waiting batch close it first).  fdk_recon_flush launches the backprojection of a
  * partial batch now (asynchronous); fdk_recon_sync and fdk_recon_get_volume flush implicitly. */
 int fdk_recon_flush(fdk_recon *h);
+/* The row filter this reconstructor runs: 0 the FFT filter (fdk_filter_*), 1 the split-FP16
+ * tensor-core GEMM (fdk_toeplitz_*, MIXED precision when nu % 256 == 0 and nv % 128 == 0 on an
+ * sm_100 GPU, unless the environment sets FDK_FILTER=fft). */
+int fdk_recon_filter_kind(fdk_recon *h, int32_t *kind);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
 /* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).

@@ -171,3 +171,28 @@ def test_batching_is_independent_of_push_pattern():
     va, vb = a.volume(), b.volume()
     assert b.stats()["views"] == views
     assert rel_l2(vb, va) <= 1e-6
+
+
+def test_tensor_core_filter_in_the_reconstructor(monkeypatch):
+    """MIXED with nu % 256 == 0 and nv % 128 == 0 filters with the split-FP16 tcgen05 GEMM; the
+    volume matches the FFT-filtered one and the FP64 pipeline."""
+    n, views = 48, 24
+    p = small_param(n, 256, 128, views)
+    p.dv = p.du = 384.0 / 256
+    _, proj = phantom_views(p, seed=5)
+    r = F.Reconstructor(p, "mixed", batch=16)
+    assert r.filter_kind == "tensor"
+    r.push(proj.copy(), 0)
+    got = r.volume()
+    monkeypatch.setenv("FDK_FILTER", "fft")
+    r2 = F.Reconstructor(p, "mixed", batch=16)
+    assert r2.filter_kind == "fft"
+    r2.push(proj.copy(), 0)
+    ref = r2.volume()
+    filt = oracle_filtered(p, proj, pad_n=4)
+    top = [0, 0, 0, n, n, n // 2]
+    f64, _ = oracle_bp_f64(top, n // 2, n, filt, p.proj_matrices(np.float64))
+    m = knife_edge_mask(p, top, n // 2)
+    e_fft, e_tc = rel_l2(ref[m], f64[m]), rel_l2(got[m], f64[m])
+    print("rel-L2 vs FP64: fft", e_fft, "tensor", e_tc, "tensor vs fft", rel_l2(got, ref))
+    assert e_tc <= 1e-3 and rel_l2(got, ref) <= 5e-4
