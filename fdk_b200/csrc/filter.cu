@@ -331,9 +331,10 @@ static int launch_mirror(const FilterArgs &a, int n_views, cudaStream_t st) {
     using P = typename PairOf<OUT>::T;
     const int np = std::min(G, std::max(1, 4096 >> a.log2W));
     const size_t smem = sizeof(float2) * np * a.W + 2 * sizeof(P) * G * a.nu;
-    if (smem > 48 * 1024)  // per device and size: cheap, so set on every launch
-        FDK_CUDA(cudaFuncSetAttribute(filter_mirror_kernel<OUT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
+    // per device and size, and needed at 48 KB too (the kernel also has static shared memory):
+    // cheap, so set on every launch
+    FDK_CUDA(cudaFuncSetAttribute(filter_mirror_kernel<OUT, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
     filter_mirror_kernel<OUT, G><<<dim3(a.nv / (2 * G), n_views), 512, smem, st>>>(a);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
@@ -353,7 +354,7 @@ static int launch_filter(const FilterArgs &a, int n_views, int layout, int dtype
     }
     const dim3 grid((a.nv + 1) / 2, n_views);
     const size_t smem = sizeof(float2) * a.W;
-    if (smem > 48 * 1024) {
+    if (smem + sizeof(float) * 4 > 48 * 1024) {  // dynamic + static (pads) above the default limit
         // opt in to more than 48 KB of dynamic shared memory (per device: set on every launch)
         FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_ROWS, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
         FDK_CUDA(cudaFuncSetAttribute(filter_rows_kernel<FDK_LAYOUT_TRANSPOSED, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));

@@ -79,3 +79,27 @@ def test_cufft_plugin_api_vs_reference(nu, nv):
     want = np.stack([O.filter_view(v, p.fft_kernel_real, p.cos_sigma, pad_n=3) for v in views.cpu().numpy()])
     assert max_rel(ref, want) <= 5e-6  # reference vs oracle
     assert max_rel(got, ref) <= 5e-6, max_rel(got, ref)
+
+
+@pytest.mark.parametrize("nu,nv", [(512, 512), (1024, 64)])
+def test_mirror_kernel_at_the_48k_shared_memory_boundary(nu, nv):
+    """nu = 512 (W = 1024, four pairs at once) and nu = 1024 (W = 2048, two pairs) put the grouped
+    MIRROR kernel at exactly 48 KiB of dynamic shared memory for FP16 and FP32 outputs."""
+    import torch
+
+    p = small_param(64, nu, nv, 2)
+    rng = np.random.default_rng(nu)
+    src = torch.from_numpy((rng.standard_normal((2, nv, nu)) * 10 + 40).astype(np.float32)).cuda()
+    eng = F.FilterEngine(p.cos_sigma, p.fft_kernel_real_f32)
+    t = torch.empty((2, nu, nv), dtype=torch.float32, device="cuda")
+    eng.run_device(src.data_ptr(), t.data_ptr(), 2, F.LAYOUT_TRANSPOSED, F.DTYPE_F32)
+    m = torch.empty((2, nu, nv, 2), dtype=torch.float32, device="cuda")
+    eng.run_device(src.data_ptr(), m.data_ptr(), 2, F.LAYOUT_MIRROR, F.DTYPE_F32)
+    h = torch.empty((2, nu, nv, 2), dtype=torch.float16, device="cuda")
+    scale = float(1.0 / p.cos_sigma.max())
+    eng.run_device(src.data_ptr(), h.data_ptr(), 2, F.LAYOUT_MIRROR, F.DTYPE_F16, scale)
+    torch.cuda.synchronize()
+    t, m = t.cpu().numpy(), m.cpu().numpy()
+    assert np.array_equal(m[..., 0], t) and np.array_equal(m[..., 1], t[:, :, ::-1])
+    hh = h.float().cpu().numpy() / scale
+    assert max_rel(hh[..., 0], t) <= 1e-3
