@@ -37,7 +37,9 @@ template <typename E>
 struct TmaCfg;
 // Tile and pipeline shapes (macros for tuning sweeps).  Measured on the 2048^3 / 4096-view
 // workload, 128 views per launch: mixed R 12 -> 16 and 4 -> 8 views per stage 1985 -> 2215 GUPS
-// (more stages changed nothing); FP32 R 8 -> 12: 1007 -> 1051 GUPS.
+// (more stages changed nothing; R >= 20 spills); FP32 R 8 -> 12: 1007 -> 1051 GUPS.  Unrolling
+// the view loop (1641 GUPS) and pairing two views per slice with an FP16 pre-add (2115 GUPS)
+// were slower: both raise register pressure past the 2-CTA budget.
 #ifndef FDK_TMA_MIXED_R
 #define FDK_TMA_MIXED_R 16
 #endif
@@ -70,9 +72,6 @@ struct TmaCfg<float2> {
     static constexpr int S = FDK_TMA_FP32_S;
 };
 
-#ifndef FDK_TMA_UNROLL_VIEWS
-#define FDK_TMA_UNROLL_VIEWS 0
-#endif
 
 constexpr long long kWaitLimit = 1ll << 26;
 constexpr unsigned long long kWaitNs = 10ull * 1000 * 1000 * 1000;  // 10 s
@@ -520,22 +519,12 @@ __global__ void __launch_bounds__(288, 2) bp_tma_kernel(const __grid_constant__ 
                 return;
             }
             if (col_ok) {
-#if FDK_TMA_UNROLL_VIEWS
-#pragma unroll
-                for (int l = 0; l < NV; l++) {
-                    const int view = c * NV + l;
-                    if (view < a.n_proj)
-                        column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + view * frame, x, y, zf0,
-                                       a.nu, a.nv, a.wscale, am, ar);
-                }
-#else
                 for (int l = 0; l < NV; l++) {
                     const int view = c * NV + l;
                     if (view >= a.n_proj) break;
                     column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + view * frame, x, y, zf0, a.nu,
                                    a.nv, a.wscale, am, ar);
                 }
-#endif
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(empty0 + 8 * s);
