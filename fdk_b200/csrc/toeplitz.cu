@@ -45,7 +45,8 @@ constexpr int A_BYTES = BM * BK * 2, B_BYTES = BN * BK * 2, STAGE_BYTES = A_BYTE
 constexpr int THREADS = 192;
 constexpr int TMEM_COLS = 512;
 constexpr unsigned long long kWaitNs = 10ull * 1000 * 1000 * 1000;
-constexpr size_t SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256;  // alignment slack + ring + barriers
+constexpr int XBUF_BYTES = 2 * 4 * 32 * 32 * 2;  // epilogue pair exchange: 2 buffers x 4 warps x 32 x 32 FP16
+constexpr size_t SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + 256 + XBUF_BYTES;  // slack, ring, barriers, exchange
 
 __device__ __forceinline__ unsigned su32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long gtime() {
@@ -133,8 +134,10 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float (&v)[32]) {
 }
 
 struct GemmArgs {
-    __half *out;        // R x N (row pitch N), FP16
-    int R, N, K;        // rows, output columns (= nu), reduction length (= nu)
+    __half *out;        // ROWS: R x N FP16 (row pitch N); MIRROR: views x N x nv FP16 pairs
+    int R, N, K;        // rows, output columns (= nu), reduction length (= nu x terms)
+    int a_cols;         // stored A columns (nu, or 2 nu for hi | lo); the K segment at 2 nu re-reads hi
+    int mirror, nv;     // MIRROR output: each 128-row tile is rows v0..v0+63 and nv-64-v0..nv-1-v0
     float out_scale;
     unsigned *err;      // device error word
     unsigned *overflow; // set when a scaled output leaves the FP16 range
@@ -156,6 +159,7 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_gemm_kernel(const __grid_
     static_assert(8 * (2 * STAGES + 5) <= 128, "barrier block");
     unsigned *tmem_word = reinterpret_cast<unsigned *>(smem + STAGES * STAGE_BYTES + 128);
     volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_word + 1);
+    unsigned *xbuf = reinterpret_cast<unsigned *>(smem + STAGES * STAGE_BYTES + 256);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int n_tiles_n = g.N / BN, n_tiles = (g.R / BM) * n_tiles_n, n_k = g.K / BK;
@@ -196,8 +200,16 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_gemm_kernel(const __grid_
                         break;
                     }
                     const unsigned sa = base + s * STAGE_BYTES, sb = sa + A_BYTES;
+                    const int xa = (kc * BK) % g.a_cols;
+                    int r0 = tm * BM, r1 = r0 + BM / 2;  // two 64-row boxes per A tile
+                    if (g.mirror) {
+                        const int blocks = g.nv / BM, f = tm / blocks, v0 = (tm % blocks) * (BM / 2);
+                        r0 = f * g.nv + v0;
+                        r1 = f * g.nv + g.nv - BM / 2 - v0;
+                    }
                     bar_expect_tx(full0 + 8 * s, STAGE_BYTES);
-                    tma_2d(sa, &map_a, kc * BK, tm * BM, full0 + 8 * s);
+                    tma_2d(sa, &map_a, xa, r0, full0 + 8 * s);
+                    tma_2d(sa + A_BYTES / 2, &map_a, xa, r1, full0 + 8 * s);
                     tma_2d(sb, &map_b, kc * BK, tn * BN, full0 + 8 * s);
                 }
             }
@@ -250,10 +262,27 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_gemm_kernel(const __grid_
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, tile_i++) {
             const int b = tile_i & 1;
             const bool ready = bar_wait(accf0 + 8 * b, (tile_i >> 1) & 1) && !*abort_flag;
-            if (!__all_sync(0xFFFFFFFFu, ready)) break;  // warp-uniform: tcgen05.ld is .sync.aligned
+            // one decision for all four epilogue warps (they meet at named barrier 1 below, and
+            // tcgen05.ld is .sync.aligned): AND-reduction over the 128 epilogue threads
+            unsigned all_ready;
+            asm volatile(
+                "{\n .reg .pred p, r;\n setp.ne.b32 p, %1, 0;\n bar.red.and.pred r, 1, 128, p;\n selp.b32 %0, 1, 0, r;\n}"
+                : "=r"(all_ready)
+                : "r"((unsigned)ready)
+                : "memory");
+            if (!all_ready) break;
             tc_fence_after();
             const int tm = t / n_tiles_n, tn = t % n_tiles_n;
+            // ROWS: this lane's output row; MIRROR: its detector row vr in view f (TMEM lanes
+            // 0..63 hold rows v0 + i, lanes 64..127 rows nv - 64 - v0 + j; lane i pairs with 127 - i)
             __half *orow = g.out + (long long)(tm * BM + row_in_tile) * g.N + tn * BN;
+            long long mbase = 0;
+            int vr = 0;
+            if (g.mirror) {
+                const int blocks = g.nv / BM, f = tm / blocks, v0 = (tm % blocks) * (BM / 2);
+                vr = row_in_tile < BM / 2 ? v0 + row_in_tile : g.nv - BM - v0 + row_in_tile;
+                mbase = (long long)f * g.N * g.nv + (long long)(tn * BN) * g.nv + vr;
+            }
 #pragma unroll 1
             for (int c = 0; c < BN / 32; c++) {
                 float v[32];
@@ -268,10 +297,29 @@ __global__ void __launch_bounds__(THREADS, 1) toeplitz_gemm_kernel(const __grid_
                     packed[i] = *reinterpret_cast<const unsigned *>(&h);
                 }
                 if (over && g.overflow) atomicOr(g.overflow, 1u);
-                uint4 *dst = reinterpret_cast<uint4 *>(orow + 32 * c);
+                if (!g.mirror) {
+                    uint4 *dst = reinterpret_cast<uint4 *>(orow + 32 * c);
 #pragma unroll
-                for (int i = 0; i < 4; i++)
-                    dst[i] = make_uint4(packed[4 * i], packed[4 * i + 1], packed[4 * i + 2], packed[4 * i + 3]);
+                    for (int i = 0; i < 4; i++)
+                        dst[i] = make_uint4(packed[4 * i], packed[4 * i + 1], packed[4 * i + 2], packed[4 * i + 3]);
+                    continue;
+                }
+                // exchange with the partner row (warp 3 - q, lane 31 - lane) through shared memory
+                unsigned *xb = xbuf + (c & 1) * (4 * 32 * 16);
+#pragma unroll
+                for (int i = 0; i < 16; i++) xb[(q * 32 + lane) * 16 + ((i + lane) & 15)] = packed[i];
+                asm volatile("bar.sync 1, 128;" ::: "memory");  // the four epilogue warps
+                const unsigned *pb = xb + ((3 - q) * 32 + (31 - lane)) * 16;
+                __half2 *dst = reinterpret_cast<__half2 *>(g.out) + mbase + (long long)(32 * c) * g.nv;
+#pragma unroll
+                for (int i = 0; i < 16; i++) {
+                    const unsigned o = packed[i], pp = pb[(i + 31 - lane) & 15];
+                    const __half2 mine = *reinterpret_cast<const __half2 *>(&o);
+                    const __half2 part = *reinterpret_cast<const __half2 *>(&pp);
+                    // element (u, vr) = (row vr, row nv-1-vr): consecutive lanes, consecutive vr
+                    dst[(long long)(2 * i) * g.nv] = __lows2half2(mine, part);
+                    dst[(long long)(2 * i + 1) * g.nv] = __highs2half2(mine, part);
+                }
             }
             tc_fence_before();
             __syncwarp();
@@ -295,41 +343,35 @@ __device__ __forceinline__ float from16(T x) {
     else return __bfloat162float(x);
 }
 
-// A operand rows: x = p * cos * in_scale (R rows of nu) as T segments of nu values each:
-// terms 1: [hi]; 2: [hi | lo]; 3: [hi | lo | hi], hi = round16(x), lo = round16(x - hi)
+// A operand rows: x = p * cos * in_scale (R rows of nu), stored as [hi] or [hi | lo] (split;
+// the GEMM's third K segment reads hi again), hi = round16(x), lo = round16(x - hi); eight
+// consecutive samples per thread (nu % 8 == 0), 128-bit loads and stores.
 template <typename T>
 __global__ void weight_convert_kernel(const float *__restrict__ src, const float *__restrict__ cos, T *__restrict__ dst,
-                                      long long n, int nu, int nv, float in_scale, int terms) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const long long row = i / nu;
+                                      long long n8, int nu, int nv, float in_scale, int split) {
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < n8; g += (long long)gridDim.x * blockDim.x) {
+        const long long i = 8 * g, row = i / nu;
         const int c = (int)(i - row * nu), v = (int)(row % nv);
-        const float x = src[i] * (cos ? cos[(long long)v * nu + c] : 1.f) * in_scale;
-        const T hi = to16<T>(x);
-        T *d = dst + row * (long long)nu * terms + c;
-        d[0] = hi;
-        if (terms > 1) d[nu] = to16<T>(x - from16<T>(hi));
-        if (terms > 2) d[2 * nu] = hi;
-    }
-}
-
-// ROWS FP16 (views x nv x nu) -> MIRROR FP16 pairs (views x nu x nv x 2)
-__global__ void rows_to_mirror_h_kernel(const __half *__restrict__ src, __half2 *__restrict__ dst, int nu, int nv) {
-    __shared__ __half tile[32][34], tilem[32][34];
-    const long long f = blockIdx.z;
-    const __half *s = src + f * (long long)nu * nv;
-    __half2 *d = dst + f * (long long)nu * nv;
-    const int u0 = blockIdx.x * 32, v0 = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int v = v0 + r, u = u0 + threadIdx.x;
-        if (u < nu && v < nv) {
-            tile[r][threadIdx.x] = s[(long long)v * nu + u];
-            tilem[r][threadIdx.x] = s[(long long)(nv - 1 - v) * nu + u];
+        const float4 *s4 = reinterpret_cast<const float4 *>(src + i);
+        const float4 *c4 = reinterpret_cast<const float4 *>(cos + (long long)v * nu + c);
+        float x[8];
+        {
+            const float4 a = s4[0], b = s4[1];
+            const float4 ca = cos ? c4[0] : make_float4(1.f, 1.f, 1.f, 1.f);
+            const float4 cb = cos ? c4[1] : make_float4(1.f, 1.f, 1.f, 1.f);
+            x[0] = a.x * ca.x * in_scale, x[1] = a.y * ca.y * in_scale, x[2] = a.z * ca.z * in_scale;
+            x[3] = a.w * ca.w * in_scale, x[4] = b.x * cb.x * in_scale, x[5] = b.y * cb.y * in_scale;
+            x[6] = b.z * cb.z * in_scale, x[7] = b.w * cb.w * in_scale;
         }
-    }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int u = u0 + r, v = v0 + threadIdx.x;
-        if (u < nu && v < nv) d[(long long)u * nv + v] = __halves2half2(tile[threadIdx.x][r], tilem[threadIdx.x][r]);
+        T hi[8], lo[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            hi[k] = to16<T>(x[k]);
+            lo[k] = to16<T>(x[k] - from16<T>(hi[k]));
+        }
+        T *d = dst + row * (long long)nu * (split ? 2 : 1) + c;
+        *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(hi);
+        if (split) *reinterpret_cast<uint4 *>(d + nu) = *reinterpret_cast<const uint4 *>(lo);
     }
 }
 
@@ -409,8 +451,7 @@ struct fdk_toeplitz {
     float m_unscale = 1.f;      // M is stored times 2^e (FP16 normal range); outputs times 2^-e
     float *d_cos = nullptr;
     void *d_M = nullptr;        // nu x nu, 16-bit
-    void *d_x = nullptr;        // views x nv x nu, 16-bit (weighted input)
-    __half *d_y = nullptr;      // views x nv x nu, FP16 rows
+    void *d_x = nullptr;        // views x nv x (nu or 2 nu), 16-bit weighted input (hi | lo)
     long long cap_views = 0;
     unsigned *d_err = nullptr;  // [0] device error word, [1] FP16 overflow
     int sms = 0;
@@ -523,34 +564,35 @@ int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst
     if (n_views > h->cap_views) {
         FDK_CUDA(cudaStreamSynchronize(st));
         if (h->d_x) cudaFree(h->d_x);
-        if (h->d_y) cudaFree(h->d_y);
         h->d_x = nullptr;
-        h->d_y = nullptr;
         h->cap_views = 0;
-        FDK_CUDA(cudaMalloc(&h->d_x, 2 * frame * n_views * h->terms));
-        FDK_CUDA(cudaMalloc((void **)&h->d_y, 2 * frame * n_views));
+        FDK_CUDA(cudaMalloc(&h->d_x, 2 * frame * n_views * (h->terms > 1 ? 2 : 1)));
         h->cap_views = n_views;
     }
-    const long long n = frame * n_views;
+    const long long n8 = frame * n_views / 8;
+    FDK_CHECK_ARG(((uintptr_t)dev_src & 15) == 0, "views must start on a 16-byte boundary");
+    const int split = h->terms > 1 ? 1 : 0;
     if (h->bf16)
         tpz::weight_convert_kernel<__nv_bfloat16><<<148 * 16, 256, 0, st>>>(
-            dev_src, h->d_cos, (__nv_bfloat16 *)h->d_x, n, h->nu, h->nv, h->in_scale, h->terms);
+            dev_src, h->d_cos, (__nv_bfloat16 *)h->d_x, n8, h->nu, h->nv, h->in_scale, split);
     else
-        tpz::weight_convert_kernel<__half><<<148 * 16, 256, 0, st>>>(dev_src, h->d_cos, (__half *)h->d_x, n, h->nu,
-                                                                     h->nv, h->in_scale, h->terms);
+        tpz::weight_convert_kernel<__half><<<148 * 16, 256, 0, st>>>(dev_src, h->d_cos, (__half *)h->d_x, n8, h->nu,
+                                                                     h->nv, h->in_scale, split);
     FDK_CUDA(cudaGetLastError());
     const long long R = (long long)h->nv * n_views;
     FDK_CHECK_ARG(R < (1ll << 31), "too many rows");
     CUtensorMap ma, mb;
-    const long long K = (long long)h->nu * h->terms;
-    FDK_TRY(encode_2d(&ma, h->d_x, R, K, tpz::BM, h->bf16));
+    const long long K = (long long)h->nu * h->terms, a_cols = (long long)h->nu * (h->terms > 1 ? 2 : 1);
+    FDK_TRY(encode_2d(&ma, h->d_x, R, a_cols, tpz::BM / 2, h->bf16));
     FDK_TRY(encode_2d(&mb, h->d_M, h->nu, K, tpz::BN, h->bf16));
     tpz::GemmArgs g;
-    __half *gout = layout == FDK_LAYOUT_ROWS ? (__half *)dev_dst : h->d_y;
-    g.out = gout;
+    g.out = (__half *)dev_dst;
     g.R = (int)R;
     g.N = h->nu;
     g.K = (int)K;
+    g.a_cols = (int)a_cols;
+    g.mirror = layout == FDK_LAYOUT_MIRROR ? 1 : 0;
+    g.nv = h->nv;
     g.out_scale = out_scale * h->m_unscale;
     g.err = h->d_err;
     g.overflow = h->d_err + 1;
@@ -561,11 +603,6 @@ int fdk_toeplitz_run_device(fdk_toeplitz *h, const float *dev_src, void *dev_dst
     else
         tpz::toeplitz_gemm_kernel<false><<<grid, tpz::THREADS, tpz::SMEM_BYTES, st>>>(ma, mb, g);
     FDK_CUDA(cudaGetLastError());
-    if (layout == FDK_LAYOUT_MIRROR) {
-        const dim3 grid2((unsigned)ceil_div(h->nu, 32), (unsigned)ceil_div(h->nv, 32), (unsigned)n_views);
-        tpz::rows_to_mirror_h_kernel<<<grid2, dim3(32, 8), 0, st>>>(h->d_y, (__half2 *)dev_dst, h->nu, h->nv);
-        FDK_CUDA(cudaGetLastError());
-    }
     return FDK_OK;
     FDK_ABI_END
 }
@@ -600,7 +637,6 @@ int fdk_toeplitz_destroy(fdk_toeplitz *h) {
     if (h->d_cos) cudaFree(h->d_cos);
     if (h->d_M) cudaFree(h->d_M);
     if (h->d_x) cudaFree(h->d_x);
-    if (h->d_y) cudaFree(h->d_y);
     if (h->d_err) cudaFree(h->d_err);
     delete h;
     return FDK_OK;
