@@ -423,7 +423,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
                 tc_peak, tc_src = mp["bf16_tflops_sustained"], "measured (cuBLAS bf16, sustained)"
             except Exception:
                 tc_peak, tc_src = 1400.0, "fallback (sustained)"
-            filter_roof = {"kernel": "toeplitz_gemm_kernel<f16> (tcgen05; + weight and layout passes)",
+            filter_roof = {"kernel": "toeplitz_gemm_kernel<f16> (tcgen05; + the weighting pass)",
                            "bound": "tensor", "achieved": flops / (flt_step_ms * 1e-3) / 1e12, "peak": tc_peak,
                            "unit": "TFLOP/s", "frac": flops / (flt_step_ms * 1e-3) / 1e12 / tc_peak,
                            "peak_source": tc_src, "algorithmic_flops_per_step": flops, "launch_ms": flt_step_ms,
@@ -442,7 +442,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "config": workload_config(param, args),
             "roofline": roofline, "filter_roofline": filter_roof,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": args.steps * (3 if filter_kind == "tensor" else 1) + n_bp_launches,
+            "gpu_launches": args.steps * (2 if filter_kind == "tensor" else 1) + n_bp_launches,
             "filter": filter_kind,
             "plain_fp32": fp32, "accuracy": acc,
         }
