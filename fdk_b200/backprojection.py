@@ -99,4 +99,14 @@ def reconstruct_conebeam(proj_size, vol_size, matrices: np.ndarray, dev_vol_in: 
     check(lib().fdk_rtk_reconstruct_conebeam(ps, vs, m.ctypes.data, dev_vol_in, dev_vol_out, p.ctypes.data))
 
 
-__all__ = ["BackProjectionFDK", "BoxT", "reconstruct_conebeam", "LAYOUT_MIRROR", "LAYOUT_TRANSPOSED"]
+def rtk_backproject_device(proj_size, vol_size, matrices: np.ndarray, dev_vol_in: int, dev_vol_out: int,
+                           dev_proj: int, stream: int = 0) -> None:
+    """The same as reconstruct_conebeam on device-resident views (up to 128), asynchronous."""
+    ps = (C.c_int32 * 3)(*proj_size)
+    vs = (C.c_int32 * 3)(*vol_size)
+    m = np.ascontiguousarray(matrices, np.float32)
+    check(lib().fdk_rtk_backproject_device(ps, vs, m.ctypes.data, dev_vol_in, dev_vol_out, dev_proj, stream))
+
+
+__all__ = ["BackProjectionFDK", "BoxT", "reconstruct_conebeam", "rtk_backproject_device", "LAYOUT_MIRROR",
+           "LAYOUT_TRANSPOSED"]

@@ -11,12 +11,17 @@
 
 namespace fdk {
 
+constexpr int kRtkMaxViews = 128;
+struct RtkMats {  // by value in the kernel parameters: no device copy per call
+    float m[kRtkMaxViews * 12];
+};
+
 __global__ void __launch_bounds__(256) rtk_bp_kernel(const float *__restrict__ vol_in, float *__restrict__ vol_out,
-                                                     const float *__restrict__ proj, const float *__restrict__ mats,
+                                                     const float *__restrict__ proj, const __grid_constant__ RtkMats mats,
                                                      int W, int H, int n, int nx, int ny, int nz) {
-    __shared__ float sm[32 * 12];
+    __shared__ float sm[kRtkMaxViews * 12];
     const int tid = threadIdx.y * 32 + threadIdx.x;
-    for (int q = tid; q < n * 12; q += 256) sm[q] = mats[q];
+    for (int q = tid; q < n * 12; q += 256) sm[q] = mats.m[q];
     __syncthreads();
     const int i = blockIdx.x * 32 + threadIdx.x;
     const int j = blockIdx.y * 8 + threadIdx.y;
@@ -51,9 +56,26 @@ __global__ void __launch_bounds__(256) rtk_bp_kernel(const float *__restrict__ v
 
 using namespace fdk;
 
-extern "C" int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_size[3],
-                                            const float *matrices, const float *dev_vol_in, float *dev_vol_out,
-                                            const float *proj) {
+namespace fdk {
+
+int rtk_launch(const int32_t proj_size[3], const int32_t vol_size[3], const float *host_mats, const float *dev_vol_in,
+               float *dev_vol_out, const float *dev_proj, cudaStream_t st) {
+    const int W = proj_size[0], H = proj_size[1], n = proj_size[2];
+    const int nx = vol_size[0], ny = vol_size[1], nz = vol_size[2];
+    RtkMats m;
+    for (int i = 0; i < 12 * n; i++) m.m[i] = host_mats[i];
+    const dim3 grid((unsigned)ceil_div(nx, 32), (unsigned)ceil_div(ny, 8), nz);
+    rtk_bp_kernel<<<grid, dim3(32, 8), 0, st>>>(dev_vol_in, dev_vol_out, dev_proj, m, W, H, n, nx, ny, nz);
+    FDK_CUDA(cudaGetLastError());
+    return FDK_OK;
+}
+
+}  // namespace fdk
+
+extern "C" {
+
+int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_size[3], const float *matrices,
+                                 const float *dev_vol_in, float *dev_vol_out, const float *proj) {
     FDK_ABI_BEGIN
     clear_error();
     FDK_CHECK_ARG(proj_size && vol_size && matrices && dev_vol_in && dev_vol_out && proj, "NULL argument");
@@ -62,21 +84,31 @@ extern "C" int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const in
     FDK_CHECK_ARG(W > 1 && H > 1 && n > 0 && n <= 32, "proj_size out of range (views <= 32)");
     FDK_CHECK_ARG(nx > 0 && ny > 0 && nz > 0 && nz <= 65535, "vol_size out of range");
     const size_t bytes = sizeof(float) * (size_t)W * H * n;
-    float *d_proj = nullptr, *d_mats = nullptr;
+    float *d_proj = nullptr;
     FDK_CUDA(cudaMalloc(&d_proj, bytes));
     int s = FDK_OK;
-    cudaError_t e = cudaMalloc(&d_mats, sizeof(float) * 12 * n);
-    if (e == cudaSuccess) e = cudaMemcpy(d_proj, proj, bytes, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(d_mats, matrices, sizeof(float) * 12 * n, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpy(d_proj, proj, bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        const dim3 grid((unsigned)ceil_div(nx, 32), (unsigned)ceil_div(ny, 8), nz);
-        rtk_bp_kernel<<<grid, dim3(32, 8)>>>(dev_vol_in, dev_vol_out, d_proj, d_mats, W, H, n, nx, ny, nz);
-        e = cudaGetLastError();
+        s = rtk_launch(proj_size, vol_size, matrices, dev_vol_in, dev_vol_out, d_proj, nullptr);
+        if (s == FDK_OK) e = cudaDeviceSynchronize();
     }
-    if (e == cudaSuccess) e = cudaDeviceSynchronize();
-    if (e != cudaSuccess) s = cuda_status(e, "CUDA_reconstruct_conebeam", __FILE__, __LINE__);
+    if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, "CUDA_reconstruct_conebeam", __FILE__, __LINE__);
     cudaFree(d_proj);
-    if (d_mats) cudaFree(d_mats);
     return s;
     FDK_ABI_END
 }
+
+int fdk_rtk_backproject_device(const int32_t proj_size[3], const int32_t vol_size[3], const float *host_mats,
+                               const float *dev_vol_in, float *dev_vol_out, const float *dev_proj, void *stream) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(proj_size && vol_size && host_mats && dev_vol_in && dev_vol_out && dev_proj, "NULL argument");
+    FDK_CHECK_ARG(proj_size[0] > 1 && proj_size[1] > 1 && proj_size[2] > 0 && proj_size[2] <= kRtkMaxViews,
+                  "proj_size out of range (views <= %d)", kRtkMaxViews);
+    FDK_CHECK_ARG(vol_size[0] > 0 && vol_size[1] > 0 && vol_size[2] > 0 && vol_size[2] <= 65535,
+                  "vol_size out of range");
+    return rtk_launch(proj_size, vol_size, host_mats, dev_vol_in, dev_vol_out, dev_proj, (cudaStream_t)stream);
+    FDK_ABI_END
+}
+
+}  // extern "C"

@@ -231,6 +231,11 @@ int fdk_bp_destroy(fdk_bp *h);
 int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_size[3],
                                  const float *matrices, const float *dev_vol_in, float *dev_vol_out,
                                  const float *proj);
+/* The same backprojection on views already in device memory (no reference counterpart): host_mats
+ * 12 floats per view, up to 128 views, dev_proj n frames of height x width (u fastest).
+ * Asynchronous on stream; vol_out may equal vol_in. */
+int fdk_rtk_backproject_device(const int32_t proj_size[3], const int32_t vol_size[3], const float *host_mats,
+                               const float *dev_vol_in, float *dev_vol_out, const float *dev_proj, void *stream);
 
 /* ---- end-to-end streaming FDK (single-GPU analogue of cuFDK's
  *      FilterThread -> BpThread handoff, cuFDK/mpiFDK.cpp:58-317) ------------- */

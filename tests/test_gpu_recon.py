@@ -134,6 +134,14 @@ def test_rtk_reconstruct_conebeam_general_geometry():
     F.reconstruct_conebeam((40, 36, views), (n, n, n), mats, vin.data_ptr(), vout.data_ptr(), proj)
     want = O.rtk_bp(proj, mats, vin.cpu().numpy())
     assert rel_l2(vout.cpu().numpy(), want) <= 1e-5
+    # the device-resident entry point: the same arithmetic on views already on the GPU
+    from fdk_b200.backprojection import rtk_backproject_device
+
+    vout2 = torch.empty_like(vin)
+    dproj = torch.from_numpy(proj).cuda()
+    rtk_backproject_device((40, 36, views), (n, n, n), mats, vin.data_ptr(), vout2.data_ptr(), dproj.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(vout, vout2)
 
 
 def test_push_folder_matches_push(tmp_path):
