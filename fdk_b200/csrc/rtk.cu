@@ -2,7 +2,7 @@
 // (cudaBP/rtkCudaFDKBackProjectionImageFilter.cu:200-330, kernel_fdk_3Dgrid :156-191,
 // RtkSUBPIXEL :83-112).
 //
-// General 3x4 geometry: every voxel evaluates the full matrix product for every view (no
+// General 3x4 geometry: every voxel evaluates its own projection for every view (no
 // circular-orbit shortcut), so tilted or non-circular trajectories are handled.  Views are
 // read from global memory through L1 with explicit FP32 bilinear interpolation (the reference
 // used point-sampled layered textures); a sample is zero outside [0, W-1) x [0, H-1).
@@ -16,6 +16,12 @@ struct RtkMats {  // by value in the kernel parameters: no device copy per call
     float m[kRtkMaxViews * 12];
 };
 
+constexpr int kRtkR = 8;  // consecutive z voxels per thread
+
+// Thread = voxel column (i, j), a run of kRtkR voxels along z.  Per view the x, y and w rows of
+// the matrix are evaluated once at z = 0 for the column; each voxel of the run adds its m[.][2] z
+// term with one FMA per row.  Four __ldg texels per sample, bilinear in FP32, zero outside
+// [0, W-1) x [0, H-1) (RtkSUBPIXEL), weight 1/w^2.
 __global__ void __launch_bounds__(256) rtk_bp_kernel(const float *__restrict__ vol_in, float *__restrict__ vol_out,
                                                      const float *__restrict__ proj, const __grid_constant__ RtkMats mats,
                                                      int W, int H, int n, int nx, int ny, int nz) {
@@ -25,31 +31,45 @@ __global__ void __launch_bounds__(256) rtk_bp_kernel(const float *__restrict__ v
     __syncthreads();
     const int i = blockIdx.x * 32 + threadIdx.x;
     const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k = blockIdx.z;
+    const int k0 = blockIdx.z * kRtkR;
     if (i >= nx || j >= ny) return;
-    const float fi = (float)i, fj = (float)j, fk = (float)k;
+    const float fi = (float)i, fj = (float)j;
+    const float wm1 = (float)(W - 1), hm1 = (float)(H - 1);
     const long long frame = (long long)W * H;
-    float acc = 0.f;
+    float acc[kRtkR];
+#pragma unroll
+    for (int kk = 0; kk < kRtkR; kk++) acc[kk] = 0.f;
     for (int p = 0; p < n; p++) {
         const float *m = sm + 12 * p;
-        const float x = fmaf(m[0], fi, fmaf(m[1], fj, fmaf(m[2], fk, m[3])));
-        const float y = fmaf(m[4], fi, fmaf(m[5], fj, fmaf(m[6], fk, m[7])));
-        const float rw = 1.0f / fmaf(m[8], fi, fmaf(m[9], fj, fmaf(m[10], fk, m[11])));
-        const float u = x * rw, v = y * rw;
-        float s = 0.f;
-        if (u >= 0.f && u < (float)(W - 1) && v >= 0.f && v < (float)(H - 1)) {
-            const float iu = floorf(u), iv = floorf(v);
-            const float du = u - iu, dv = v - iv;
-            const float *p0 = proj + p * frame + (long long)iv * W + (int)iu;
-            const float *p1 = p0 + W;
-            const float a = fmaf(du, __ldg(p0 + 1) - __ldg(p0), __ldg(p0));
-            const float b = fmaf(du, __ldg(p1 + 1) - __ldg(p1), __ldg(p1));
-            s = fmaf(dv, b - a, a);
+        const float X = fmaf(m[0], fi, fmaf(m[1], fj, m[3]));
+        const float Y = fmaf(m[4], fi, fmaf(m[5], fj, m[7]));
+        const float Z = fmaf(m[8], fi, fmaf(m[9], fj, m[11]));
+        const float *pv = proj + p * frame;
+#pragma unroll
+        for (int kk = 0; kk < kRtkR; kk++) {
+            const float fk = (float)(k0 + kk);
+            const float rw = __fdividef(1.0f, fmaf(m[10], fk, Z));
+            const float u = fmaf(m[2], fk, X) * rw, v = fmaf(m[6], fk, Y) * rw;
+            float s = 0.f;
+            if (u >= 0.f && u < wm1 && v >= 0.f && v < hm1) {
+                const float iu = floorf(u), iv = floorf(v);
+                const float du = u - iu, dv = v - iv;
+                const float *p0 = pv + (long long)iv * W + (int)iu;
+                const float *p1 = p0 + W;
+                const float a = fmaf(du, __ldg(p0 + 1) - __ldg(p0), __ldg(p0));
+                const float b = fmaf(du, __ldg(p1 + 1) - __ldg(p1), __ldg(p1));
+                s = fmaf(dv, b - a, a);
+            }
+            acc[kk] = fmaf(s * rw, rw, acc[kk]);
         }
-        acc = fmaf(s * rw, rw, acc);
     }
-    const long long idx = i + ((long long)j + (long long)k * ny) * nx;
-    vol_out[idx] = vol_in[idx] + acc;
+#pragma unroll
+    for (int kk = 0; kk < kRtkR; kk++) {
+        const int k = k0 + kk;
+        if (k >= nz) break;
+        const long long idx = i + ((long long)j + (long long)k * ny) * nx;
+        vol_out[idx] = vol_in[idx] + acc[kk];
+    }
 }
 
 }  // namespace fdk
@@ -64,7 +84,7 @@ int rtk_launch(const int32_t proj_size[3], const int32_t vol_size[3], const floa
     const int nx = vol_size[0], ny = vol_size[1], nz = vol_size[2];
     RtkMats m;
     for (int i = 0; i < 12 * n; i++) m.m[i] = host_mats[i];
-    const dim3 grid((unsigned)ceil_div(nx, 32), (unsigned)ceil_div(ny, 8), nz);
+    const dim3 grid((unsigned)ceil_div(nx, 32), (unsigned)ceil_div(ny, 8), (unsigned)ceil_div(nz, kRtkR));
     rtk_bp_kernel<<<grid, dim3(32, 8), 0, st>>>(dev_vol_in, dev_vol_out, dev_proj, m, W, H, n, nx, ny, nz);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
