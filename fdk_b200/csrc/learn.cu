@@ -1,7 +1,7 @@
 // learn.cu -- the learned residual row filter and what training it needs (no reference
-// counterpart: "a small 1D residual filter network (3 conv layers, 32
-// channels, kernel 9) refines each ramp-filtered row ... trained on phantoms the project's own
-// ray-marching forward projector generates, and backpropagates through BP").
+// counterpart): a small 1D residual network (3 conv layers, 32 channels, kernel 9) refines each
+// ramp-filtered row; it is trained on phantoms that this library's own ray-marching forward
+// projector generates, with the loss backpropagated through the exact adjoint of BP.
 //
 // Network, per detector row x (length L = nu), s = the row scale (1 / (SOD^2 AAF): line-integral
 // units):

@@ -9,8 +9,8 @@
 // (off = (W - nu) / 2; the pads are means of the first / last pad_n samples, Filterlib/
 // FilterLib.h:26-46 and cudaFftFilter.cu kernelPad).  M is built once in FP64 on the host and
 // stored FP16 or BF16; a batch of views is then one GEMM  Y[R][nu] = X[R][nu] . M^T  with R =
-// views x nv rows, FP16/BF16 operands and FP32 accumulation (north star: "a Toeplitz row-GEMM on
-// the tensor cores (BF16 in, FP32 accumulate)").  The ramp filter cancels most of its input, so
+// views x nv rows, FP16/BF16 operands and FP32 accumulation (a Toeplitz row-GEMM on the tensor
+// cores).  The ramp filter cancels most of its input, so
 // 16-bit input rounding shows up ~10x larger in its output; the split mode keeps the operands'
 // low parts too, x = x_hi + x_lo and M = M_hi + M_lo, and sums x_hi M_hi + x_lo M_hi + x_hi M_lo
 // in the same GEMM with K = 3 nu (three times the FLOPs, close to FP32 accuracy).

@@ -13,7 +13,7 @@ through the exact backprojection adjoint (fdk_bp_adjoint) and the network's back
 Adam (lr 1e-3, cosine-decayed to 1e-5 over the run by default).  Every kernel is this library's
 own (learn.cu, fproj.cu, filter.cu, bp_tma.cuh).
 
-Plain Hann-ramp FDK (zero residual) is the fallback and the judge: on each held-out scan the
+Plain Hann-ramp FDK (zero residual) is the fallback and the referee: on each held-out scan the
 learned reconstruction is kept only when its error against the phantom is lower.
 """
 from __future__ import annotations
@@ -59,7 +59,7 @@ class Pipeline:
 
     input_window: the ramp-filter window of the rows the network reads ("hann", the geometry's
     own, or e.g. "ram-lak" to let the network learn its own apodization).  Plain FDK, the
-    fallback and judge, always uses the geometry's window."""
+    fallback and referee, always uses the geometry's window."""
 
     def __init__(self, param=None, device: int = 0, input_window: str | None = None):
         import torch
@@ -201,7 +201,7 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
 
 
 def evaluate(params, n_test: int = 200, seed0: int = 5000, input_window: str | None = None) -> dict:
-    """Held-out scans: MSE of plain FDK, of the learned filter, and of the judged choice."""
+    """Held-out scans: MSE of plain FDK, of the learned filter, and of the gated choice."""
     import torch
 
     pl = Pipeline(input_window=input_window)

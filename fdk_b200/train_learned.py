@@ -1,10 +1,10 @@
-"""Train and judge the learned residual row filter on the C5 workload.
+"""Train and evaluate the learned residual row filter on the C5 workload.
 
     python -m fdk_b200.train_learned [--n-train 2000] [--epochs 20] [--n-test 200]
                                       [--time-limit S] [--out fdk_b200/weights/residual_c5.npz]
 
 Writes the trained parameters (npz) and prints one JSON line with the held-out result: MSE of
-plain Hann-ramp FDK, of the learned filter, and of the judged choice (the learned reconstruction
+plain Hann-ramp FDK, of the learned filter, and of the gated choice (the learned reconstruction
 kept only where it beats plain FDK against the phantom), plus the training history.
 """
 from __future__ import annotations

@@ -131,8 +131,8 @@ int fdk_filter_run_device(fdk_filter *h, const float *src_dev, void *dst_dev, in
                           int32_t layout, int32_t out_dtype, float out_scale, void *stream);
 int fdk_filter_destroy(fdk_filter *h);
 
-/* The same filter as a GEMM on the tensor cores (no reference counterpart; the north star's
- * "Toeplitz row-GEMM ... BF16 in, FP32 accumulate").  Per row, y = M (in_scale * cos * p) with M
+/* The same filter as a GEMM on the tensor cores (no reference counterpart: a Toeplitz
+ * row-GEMM, 16-bit operands, FP32 accumulation).  Per row, y = M (in_scale * cos * p) with M
  * the nu x nu matrix of the fused filter (edge-mean pads, circular kernel IDFT(H), crop; built in
  * FP64, stored FP16 or BF16 when bf16 != 0).  split != 0 keeps the low parts of both operands
  * (x_hi M_hi + x_lo M_hi + x_hi M_lo, three times the FLOPs, close to FP32 accuracy).  nu must be

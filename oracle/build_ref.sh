@@ -7,7 +7,7 @@
 # with the rest of the tree).  Nothing from the reference tree is copied into the
 # repository.  The reference's own build system (VisualGDB makefiles) is not used.
 #
-# Two build-time adjustments, both recorded in DESIGN.md:
+# Two build-time adjustments:
 #  1. common/type.h:3144 needs the `template` disambiguator under g++ (MSVC accepts
 #     `x.FilterX<D>(...)` on a dependent expression).  A sed-fixed copy is generated
 #     into oracle/_ref/gen/ and force-included first; its include guard (__Type_H)
