@@ -1,9 +1,14 @@
 // recon.cu -- end-to-end streaming FDK on one GPU: the single-GPU analogue of cuFDK's
 // FilterThread -> BpThread handoff (cuFDK/mpiFDK.cpp:58-317).
 //
-//   host views --(copy stream, 2 staging slots)--> raw views on the device
+//   host views --(copy stream, a ring of raw-view slots)--> raw views on the device
 //   --(compute stream)--> fused cosine weight + ramp filter, written straight into the
 //   backprojection's layout --> backprojection into the resident volume.
+//
+// Views move in chunks of up to 32; the ring holds batch / chunk + 2 chunks, so the copies of
+// the next batch's views land while the current batch's backprojection runs (a slot is free
+// again once its chunk is filtered, and the filters of a batch queue behind the previous
+// batch's backprojection on the compute stream).
 //
 // The whole volume is one mirror-symmetric slab pair (DivVolume with one rank,
 // cuFDK/mpiFDK.h:116-149): top = z in [0, nz/2), bottom = z in [nz/2, nz).  Host waits are
@@ -33,7 +38,8 @@ struct fdk_recon {
     FilterTables tables;
     float *d_cos = nullptr;
     fdk_toeplitz *tpz = nullptr;     // tensor-core filter (MIXED), else the FFT filter
-    float *d_raw[2] = {nullptr, nullptr};
+    int chunk = 32;                  // views per raw slot
+    std::vector<float *> d_raw;      // the ring of raw-view slots
     void *d_filt = nullptr;
     float *d_scale = nullptr;        // accumulator scale of FP16 views (device scalar)
     unsigned int *d_overflow = nullptr;
@@ -41,7 +47,7 @@ struct fdk_recon {
     std::vector<float> mats;         // 12 x n_proj, FP32 (from FP64)
     float *d_mats = nullptr;         // the same on the device
     cudaStream_t compute = nullptr, copy = nullptr;
-    cudaEvent_t raw_ready[2] = {nullptr, nullptr}, raw_free[2] = {nullptr, nullptr};
+    std::vector<cudaEvent_t> raw_ready, raw_free;
     cudaEvent_t f0 = nullptr, f1 = nullptr, done = nullptr;
     int slot = 0;
     // filtered views waiting in d_filt for a full batch: views pend_first .. pend_first+pending-1
@@ -50,7 +56,7 @@ struct fdk_recon {
     double filter_ms = 0;
     long long views = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
-    // pinned staging of fdk_recon_push_folder (allocated on first use): two batches
+    // pinned staging of fdk_recon_push_folder (allocated on first use): two chunks
     float *h_stage[2] = {nullptr, nullptr};
     cudaEvent_t stage_free[2] = {nullptr, nullptr};
 };
@@ -73,10 +79,13 @@ int recon_release(fdk_recon *h) {
     for (int i = 0; i < 2; i++) {
         if (h->h_stage[i]) cudaFreeHost(h->h_stage[i]);
         if (h->stage_free[i]) cudaEventDestroy(h->stage_free[i]);
-        if (h->d_raw[i]) cudaFree(h->d_raw[i]);
-        if (h->raw_ready[i]) cudaEventDestroy(h->raw_ready[i]);
-        if (h->raw_free[i]) cudaEventDestroy(h->raw_free[i]);
     }
+    for (float *p : h->d_raw)
+        if (p) cudaFree(p);
+    for (cudaEvent_t e : h->raw_ready)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->raw_free)
+        if (e) cudaEventDestroy(e);
     for (auto &t : h->ftimers) {
         cudaEventDestroy(t.first);
         cudaEventDestroy(t.second);
@@ -106,7 +115,6 @@ int collect_filter_timers(fdk_recon *h) {
     return FDK_OK;
 }
 
-// Filter + backproject views [first, first+n) whose raw data is at d_src (nv x nu each).
 // Backproject the filtered views waiting in d_filt (one launch), on the compute stream.
 int flush_pending(fdk_recon *h) {
     if (h->pending == 0) return FDK_OK;
@@ -126,6 +134,7 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
     const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
     if (h->pending > 0 && first != h->pend_first + h->pending) FDK_TRY(flush_pending(h));
     for (int done = 0; done < n;) {
+        if (h->pending == h->batch) FDK_TRY(flush_pending(h));
         if (h->pending == 0) h->pend_first = first + done;
         const int m = std::min(n - done, h->batch - h->pending);
         void *dst = static_cast<unsigned char *>(h->d_filt) + (size_t)h->pending * dstride * esz;
@@ -144,10 +153,11 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
         h->ftimers.push_back(t);
         h->pending += m;
         done += m;
-        if (h->pending == h->batch) FDK_TRY(flush_pending(h));
     }
     if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
+    // the raw views are consumed once filtered: release them before a full batch's launch
     if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
+    if (h->pending == h->batch) FDK_TRY(flush_pending(h));
     h->views += n;
     return FDK_OK;
 }
@@ -209,8 +219,13 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
     if (s == FDK_OK) ck(cudaMalloc(&h->d_mats, sizeof(float) * h->mats.size()), "matrices");
     if (s == FDK_OK)
         ck(cudaMemcpy(h->d_mats, h->mats.data(), sizeof(float) * h->mats.size(), cudaMemcpyHostToDevice), "matrices");
-    for (int i = 0; i < 2 && s == FDK_OK; i++) {
-        ck(cudaMalloc(&h->d_raw[i], sizeof(float) * frame * batch), "raw views");
+    h->chunk = std::min(batch, 32);
+    const int n_slots = (batch + h->chunk - 1) / h->chunk + 2;
+    h->d_raw.assign(n_slots, nullptr);
+    h->raw_ready.assign(n_slots, nullptr);
+    h->raw_free.assign(n_slots, nullptr);
+    for (int i = 0; i < n_slots && s == FDK_OK; i++) {
+        ck(cudaMalloc(&h->d_raw[i], sizeof(float) * frame * h->chunk), "raw views");
         ck(cudaEventCreateWithFlags(&h->raw_ready[i], cudaEventDisableTiming), "event");
         ck(cudaEventCreateWithFlags(&h->raw_free[i], cudaEventDisableTiming), "event");
     }
@@ -271,12 +286,12 @@ int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
     const long long frame = h->g.nu * h->g.nv;
-    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    const int cap = h->chunk;
     cudaEvent_t last = nullptr;
     for (long long c = 0; c < n; c += cap) {
         const int m = (int)std::min<long long>(cap, n - c);
         const int k = h->slot;
-        h->slot ^= 1;
+        h->slot = (k + 1) % (int)h->d_raw.size();
         FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
         FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], host_views + c * frame, sizeof(float) * frame * m,
                                  cudaMemcpyHostToDevice, h->copy));
@@ -303,7 +318,7 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
     FDK_TRY(dg.status);
     const int nu = (int)h->g.nu, nv = (int)h->g.nv;
     const long long frame = (long long)nu * nv;
-    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    const int cap = h->chunk;
     // sizes of every file first, as the reference's folder loader
     for (long long i = 0; i < n; i++) {
         const std::string p = proj_file_path(folder, (first + i) * step + start);
@@ -333,7 +348,7 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
         FDK_CUDA(cudaEventSynchronize(h->stage_free[b]));  // staging b's previous copy has landed
         FDK_TRY(read_views(folder, nu, nv, first + c, m, step, start, h->h_stage[b], threads));
         const int k = h->slot;
-        h->slot ^= 1;
+        h->slot = (k + 1) % (int)h->d_raw.size();
         FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
         FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], h->h_stage[b], sizeof(float) * frame * m, cudaMemcpyHostToDevice,
                                  h->copy));
