@@ -5,7 +5,10 @@ per variant the time per batch of views (CUDA events, inputs resident in HBM), H
 algorithmic bytes, GEMM TFLOP/s, and rel-L2 / max error of the filtered rows against the FP64
 oracle on the first view.  One JSON line.
 
-  python -m fdk_b200.filter_bench [c4|c3] [batch] [reps]
+  python -m fdk_b200.filter_bench [c4|c3] [batch] [reps] [variant,...]
+
+The optional last argument keeps only the named variants (fft, toeplitz_f16, toeplitz_bf16,
+toeplitz_f16_split, toeplitz_bf16_split), e.g. to profile one kernel.
 """
 import json
 import os
@@ -23,6 +26,8 @@ def main():
     cfg = sys.argv[1] if len(sys.argv) > 1 else "c4"
     batch = int(sys.argv[2]) if len(sys.argv) > 2 else 128
     reps = int(sys.argv[3]) if len(sys.argv) > 3 else 5
+    only = set(sys.argv[4].split(",")) if len(sys.argv) > 4 else None
+    keep = lambda name: only is None or name in only  # noqa: E731
     p = F.config(cfg)
     nu, nv = p.nu, p.nv
     s = float(1.0 / (p.SOD * p.SOD * p.AngularAndrampFactor))
@@ -54,17 +59,21 @@ def main():
         return {"rel_l2": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
                 "max_rel": float(np.abs(got - want).max() / np.abs(want).max())}
 
-    eng = F.FilterEngine(p.cos_sigma, p.fft_kernel_real_f32, pad_edge=4)
-    ms = timed(lambda: eng.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, F.DTYPE_F16, s))
-    hbm = batch * frame * (4 + 4)
-    res["variants"]["fft"] = {"ms": ms, "hbm_gbs": hbm / (ms * 1e-3) / 1e9, **errors(out)}
+    if keep("fft"):
+        eng = F.FilterEngine(p.cos_sigma, p.fft_kernel_real_f32, pad_edge=4)
+        ms = timed(lambda: eng.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, F.DTYPE_F16, s))
+        hbm = batch * frame * (4 + 4)
+        res["variants"]["fft"] = {"ms": ms, "hbm_gbs": hbm / (ms * 1e-3) / 1e9, **errors(out)}
     flops = 2.0 * batch * nv * nu * nu
     for dt, split in (("f16", False), ("bf16", False), ("f16", True), ("bf16", True)):
+        name = f"toeplitz_{dt}{'_split' if split else ''}"
+        if not keep(name):
+            continue
         tf = F.ToeplitzFilter(p.cos_sigma, p.fft_kernel_real, 4, dt, in_scale=s, split=split)
         ms = timed(lambda: tf.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, 1.0))
         tf.check()
         terms = 3 if split else 1
-        res["variants"][f"toeplitz_{dt}{'_split' if split else ''}"] = {
+        res["variants"][name] = {
             "ms": ms, "tflops": terms * flops / (ms * 1e-3) / 1e12, **errors(out)}
         tf.close()
     print(json.dumps(res), flush=True)
