@@ -168,10 +168,10 @@ BATCH = 128  # views per backprojection launch (every fourth step)
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
-def count_bp_launches(firsts, n: int) -> int:
-    """Backprojection launches the reconstructor makes for pushes of n views starting at `firsts`
-    (from an empty batch, flushed at the end): a launch per full batch, per push that does not
-    continue the waiting batch, and the final flush."""
+def count_bp_batches(firsts, n: int) -> int:
+    """Backprojection batches the reconstructor runs for pushes of n views starting at `firsts`
+    (from an empty batch, flushed at the end): one per full batch, per push that does not
+    continue the waiting batch, and the final flush.  A batch is one kernel launch per z band."""
     pending, pf, launches = 0, 0, 0
     for f in firsts:
         if pending and f != pf + pending:
@@ -198,14 +198,14 @@ def workload_config(param, args) -> dict:
 
 
 def read_traffic(name: str):
-    """DRAM bytes per launch recorded from an ncu capture (profiles/<name>.md line
-    'dram_bytes_per_launch_full: X')."""
+    """DRAM bytes per backprojection batch (or filter launch) recorded from an ncu capture
+    (profiles/<name>.md line 'dram_bytes_per_batch_full: X' or 'dram_bytes_per_launch_full: X')."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         txt = open(path).read()
     except OSError:
         return None
-    m = re.search(r"dram_bytes_per_launch_full:\s*([0-9.eE+]+)", txt)
+    m = re.search(r"dram_bytes_per_(?:launch|batch)_full:\s*([0-9.eE+]+)", txt)
     return float(m.group(1)) if m else None
 
 
@@ -268,6 +268,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             r.push_device(ptr, first, B)
         r.sync()
         st0 = r.stats()
+        l0 = r.launch_count
         barrier()
         stream = torch.cuda.ExternalStream(r.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -281,17 +282,17 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         ms = e0.elapsed_time(e1)
         barrier()
         st1 = r.stats()
-        return r, ms, st1["bp_ms"] - st0["bp_ms"], st1["filter_ms"] - st0["filter_ms"]
+        return r, ms, st1["bp_ms"] - st0["bp_ms"], st1["filter_ms"] - st0["filter_ms"], r.launch_count - l0
 
     upd_step_all = param.nx * param.ny * param.nz * B          # whole volume, all ranks
     upd_step_rank = param.nx * param.ny * 2 * slab[1] * B      # this rank's slab pair
     clocks = ClockSampler(local)
     clocks.start()
-    r, ms, bp_ms, flt_ms = timed_device_run(args.precision, args.steps, args.warmup)
+    r, ms, bp_ms, flt_ms, n_launches = timed_device_run(args.precision, args.steps, args.warmup)
     filter_kind = r.filter_kind
     clk = clocks.stop()
     ms_max = allmax(ms)
-    n_bp_launches = count_bp_launches([batch_of(b)[1] for b in range(args.warmup, args.warmup + args.steps)], B)
+    n_bp_batches = count_bp_batches([batch_of(b)[1] for b in range(args.warmup, args.warmup + args.steps)], B)
     value = upd_step_all * args.steps / (ms_max * 1e-3) / 1e9
     kernel_gups = upd_step_rank * args.steps / (bp_ms * 1e-3) / 1e9
     log(f"{args.precision}: {ms / args.steps:.2f} ms/step, {value:.1f} GUPS (BP kernels {kernel_gups:.1f} GUPS, "
@@ -321,7 +322,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         del r
         torch.cuda.empty_cache()
         ks = max(4, args.steps // 8)
-        r2, ms2, bp2, _ = timed_device_run("fp32", ks, 2)
+        r2, ms2, bp2, _, _ = timed_device_run("fp32", ks, 2)
         v2 = upd_step_all * ks / (allmax(ms2) * 1e-3) / 1e9
         fp32 = {"value": v2, "unit": "GUPS", "steps": ks, "bp_kernel_gups": upd_step_rank * ks / (bp2 * 1e-3) / 1e9,
                 "speedup_mixed_over_fp32": value / v2}
@@ -389,7 +390,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         peak_smem = peaks["smem_gbs"] * 1e9 / bpu / 1e9
         peak_fma = peaks["fp32_tflops"] * 1e12 / 2 / fpu / 1e9
         peak = min(peak_smem, peak_fma)
-        hbm_bytes_launch = (param.nx * param.ny * 2 * slab[1] * (16 if args.precision == "mixed" else 8)
+        hbm_bytes_batch = (param.nx * param.ny * 2 * slab[1] * (16 if args.precision == "mixed" else 8)
                             + BATCH * frame * (4 if args.precision == "mixed" else 8))
         mp = {}
         try:
@@ -397,7 +398,8 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             hbm_peak, hbm_src = mp["hbm_gbs"], "measured"
         except Exception:
             hbm_peak, hbm_src = 6650.0, "fallback"
-        bp_launch_ms = bp_ms / n_bp_launches
+        bp_batch_ms = bp_ms / n_bp_batches
+        bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / n_bp_batches
         traffic = read_traffic(f"bp_tma_{args.precision}_c2.md")
         roofline = {
             "kernel": f"bp_tma_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
@@ -408,10 +410,11 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "peak_source": (f"measured on this GPU by fdk_probe_smem ({peaks['smem_gbs']:.0f} GB/s) / {bpu} B "
                             f"per update and fdk_probe_fma ({peaks['fp32_tflops']:.1f} TFLOP/s) / {fpu} FMA per "
                             "update"),
-            "launch_ms": bp_launch_ms,
-            "hbm": {"achieved": hbm_bytes_launch / (bp_launch_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": hbm_bytes_launch / (bp_launch_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
-                    "algorithmic_bytes_per_launch": hbm_bytes_launch},
+            "batch_ms": bp_batch_ms,
+            "batch": f"{BATCH} views over the whole volume, run as {bands:g} launches over z bands",
+            "hbm": {"achieved": hbm_bytes_batch / (bp_batch_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_bytes_batch / (bp_batch_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
+                    "algorithmic_bytes_per_batch": hbm_bytes_batch},
         }
         out_b = 4 if args.precision == "mixed" else 8
         flt_bytes = B * frame * (4 + out_b)
@@ -442,7 +445,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "config": workload_config(param, args),
             "roofline": roofline, "filter_roofline": filter_roof,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": args.steps * (2 if filter_kind == "tensor" else 1) + n_bp_launches,
+            "gpu_launches": n_launches,
             "filter": filter_kind,
             "plain_fp32": fp32, "accuracy": acc,
         }

@@ -43,7 +43,7 @@ EXPORTED = [
     "fdk_rtk_reconstruct_conebeam", "fdk_rtk_backproject_device",
     "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device",
     "fdk_recon_push_folder", "fdk_recon_flush", "fdk_recon_filter_kind", "fdk_recon_sync",
-    "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_reset", "fdk_recon_destroy",
+    "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_launch_count", "fdk_recon_reset", "fdk_recon_destroy",
     "fdk_phantom_project", "fdk_forward_project", "fdk_probe_smem", "fdk_probe_fma",
     "fdk_nn_param_count", "fdk_nn_forward", "fdk_nn_backward", "fdk_adam_step", "fdk_transmission_noise",
     "fdk_voxelize", "fdk_rows_to_mirror", "fdk_volume_mse", "fdk_bp_adjoint",
@@ -142,6 +142,7 @@ def lib() -> C.CDLL:
         "fdk_recon_sync": ([vp, i64], C.c_int),
         "fdk_recon_get_volume": ([vp, vp, i64], C.c_int),
         "fdk_recon_stats": ([vp, f64p, f64p, C.POINTER(i64)], C.c_int),
+        "fdk_recon_launch_count": ([vp, C.POINTER(i64)], C.c_int),
         "fdk_recon_reset": ([vp], C.c_int),
         "fdk_recon_destroy": ([vp], C.c_int),
         "fdk_phantom_project": ([G, vp, i32, i64, i64, vp, vp], C.c_int),

@@ -19,45 +19,47 @@
 namespace fdk {
 
 // [x][y][zs] -> [zs][y][x] for zs in [z_begin, z_begin + dz), x fastest
-// (kernelTransformVolume, backprojectionFDK.cu:131-148).
-__global__ void transform_volume_kernel(const float *__restrict__ src, float *__restrict__ dst, int nxs, int nys,
-                                        long long D, long long z_begin, int dz) {
+// (kernelTransformVolume, backprojectionFDK.cu:131-148).  One warp per block walks 32 x 32
+// (x, zs) tiles grid-stride.  A readback runs beside the persistent backprojection, whose
+// warps leave each SM sub-partition room for about one more warp of 32 registers: single-warp
+// blocks capped at 32 registers fit there, larger blocks wait for the backprojection to end.
+template <bool COMP>
+__global__ void __maxnreg__(32) transform_volume_kernel(const float *__restrict__ src, const float *__restrict__ comp,
+                                                      float *__restrict__ dst, int nxs, int nys, long long D,
+                                                      long long z_begin, int dz) {
     __shared__ float tile[32][33];
-    const int x0 = blockIdx.x * 32, z0 = blockIdx.z * 32;
-    const int y = blockIdx.y;
-    // read: consecutive threads walk zs (contiguous in src)
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int x = x0 + r, z = z0 + threadIdx.x;
-        if (x < nxs && z < dz) tile[r][threadIdx.x] = src[((long long)x * nys + y) * D + z_begin + z];
+    const int lane = threadIdx.x;
+    const int ntx = (nxs + 31) / 32, ntz = (dz + 31) / 32;
+    const long long n_tiles = (long long)ntx * ntz * nys;
+    const long long xs = (long long)nys * D, zs = (long long)nys * nxs;  // strides of x in src, z in dst
+    for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        const int x0 = (int)(t % ntx) * 32;
+        const long long r = t / ntx;
+        const int z0 = (int)(r % ntz) * 32, y = (int)(r / ntz);
+        const int nx = min(32, nxs - x0), nz = min(32, dz - z0);
+        // read: lanes walk zs (contiguous in src)
+        if (lane < nz) {
+            const long long o = ((long long)x0 * nys + y) * D + z_begin + z0 + lane;
+            const float *s = src + o;
+            const float *c = COMP ? comp + o : nullptr;
+#pragma unroll 4
+            for (int row = 0; row < nx; row++, s += xs) {
+                if (COMP) {
+                    tile[row][lane] = *s - *c;  // MIXED folds its compensation
+                    c += xs;
+                } else {
+                    tile[row][lane] = *s;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < nx) {
+            float *d = dst + ((long long)z0 * nys + y) * nxs + x0 + lane;
+#pragma unroll 4
+            for (int row = 0; row < nz; row++, d += zs) *d = tile[lane][row];
+        }
+        __syncwarp();
     }
-    __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
-        const int z = z0 + r, x = x0 + threadIdx.x;
-        if (x < nxs && z < dz) dst[((long long)z * nys + y) * nxs + x] = tile[threadIdx.x][r];
-    }
-}
-
-int transform_volume_to_host(const float *d_vol, int nxs, int nys, long long D, float *host, cudaStream_t st) {
-    // chunk of z slices staged through a bounded device buffer
-    const long long plane = (long long)nxs * nys;
-    long long dz = (256ll << 20) / (plane * 4);
-    if (dz < 1) dz = 1;
-    if (dz > D) dz = D;
-    float *tmp = nullptr;
-    FDK_CUDA(cudaMalloc(&tmp, sizeof(float) * plane * dz));
-    int s = FDK_OK;
-    for (long long z = 0; z < D && s == FDK_OK; z += dz) {
-        const int n = (int)std::min(dz, D - z);
-        const dim3 grid((unsigned)ceil_div(nxs, 32), nys, (unsigned)ceil_div(n, 32));
-        transform_volume_kernel<<<grid, dim3(32, 8), 0, st>>>(d_vol, tmp, nxs, nys, D, z, n);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(host + plane * z, tmp, sizeof(float) * plane * n, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) s = cuda_status(e, "GetVolumeData", __FILE__, __LINE__);
-    }
-    cudaFree(tmp);
-    return s;
 }
 
 // TRANSPOSED f32 views (height = nu rows of width = nv) -> MIRROR pairs (u, v) = (v, nv-1-v).
@@ -133,6 +135,10 @@ __global__ void transpose_views_kernel(const float *__restrict__ src, float *__r
 
 using namespace fdk;
 
+namespace {
+constexpr int kMaxBands = 4;
+}
+
 struct fdk_bp {
     int device = 0, precision = FDK_BP_FP32_EXACT;
     int proj_w = 0, proj_h = 0, proj_count = 0;
@@ -154,6 +160,17 @@ struct fdk_bp {
     BpFastPlan plan;
     unsigned int *d_absmax = nullptr;
     const float *ext_scale = nullptr;  // accumulator scale of FP16 views pushed by the reconstructor
+    // The staged kernel runs each batch as n_bands launches over bands of z tiles (top slices
+    // [band_z[k], band_z[k+1]) with their mirrors), each recording band_done[k]; a readback
+    // copies band k to the host while the later bands of the last batch still run.
+    int n_bands = 1;
+    long long band_z[kMaxBands + 1] = {};
+    int band_tz[kMaxBands + 1] = {};          // the same bounds in z tiles of the staged kernel
+    cudaEvent_t band_done[kMaxBands] = {};
+    cudaStream_t rb[2] = {nullptr, nullptr};  // readback streams
+    float *d_rb = nullptr;                    // readback staging, 2 x rb_planes z planes
+    long long rb_planes = 0;
+    long long launches = 0;                   // kernel launches since creation or reset
 };
 
 namespace bpi {
@@ -217,19 +234,27 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
         else if (transpose) bp_exact_kernel<false, true><<<grid, dim3(32, 8), 0, st>>>(a);
         else bp_exact_kernel<false, false><<<grid, dim3(32, 8), 0, st>>>(a);
         FDK_CUDA(cudaGetLastError());
+        h->launches++;
+        for (int k = 0; k < h->n_bands; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
     } else {
         FDK_CHECK_ARG(layout == FDK_LAYOUT_MIRROR, "fast backprojection reads the MIRROR layout");
         if (h->plan.tma_ok && ((uintptr_t)dev_proj & 15) == 0) {
-            if (h->precision == FDK_BP_MIXED)
-                FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
-                                               acc_scale));
-            else
-                FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
-                                              acc_scale));
+            for (int k = 0; k < h->n_bands; k++) {
+                if (h->precision == FDK_BP_MIXED)
+                    FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
+                                                   acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                else
+                    FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
+                                                  acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                h->launches++;
+                FDK_CUDA(cudaEventRecord(h->band_done[k], st));
+            }
         } else {
             const float ws = weight_scale(host_mats, h->top.x + 0.5f * (h->top.width - 1),
                                           h->top.y + 0.5f * (h->top.height - 1));
             FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, ws, acc_scale));
+            h->launches++;
+            for (int k = 0; k < h->n_bands; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
         }
     }
     FDK_CUDA(cudaEventRecord(tm.second, st));
@@ -247,6 +272,54 @@ int check_device_error(fdk_bp *h) {
         cudaMemset(h->plan.d_err, 0, sizeof(e));
         return fail(FDK_ERR_DEVICE_CHECK, "backprojection pipeline wait timed out on the device (error word %u)", e);
     }
+    return FDK_OK;
+}
+
+// Volume -> host as [zs][y][x], band by band: each chunk of z planes waits only for the launch
+// of its band (the band events of the latest batch), so the copies of the first bands overlap
+// the backprojection of the later ones.  Two streams alternate over two staging buffers; the
+// MIXED compensation is folded in on the way out (the device state keeps both terms).
+int read_volume(fdk_bp *h, float *host) {
+    const int nxs = (int)h->top.width, nys = (int)h->top.height;
+    const long long plane = (long long)nxs * nys, D = h->D, dz = h->rb_planes;
+    struct Range {
+        long long z, n;
+        int band;
+    };
+    std::vector<Range> ranges;
+    if (h->n_bands == 1) {
+        ranges.push_back({0, D, 0});
+    } else {
+        for (int k = 0; k < h->n_bands; k++) {
+            const long long za = h->band_z[k], zb = h->band_z[k + 1];
+            ranges.push_back({za, zb - za, k});          // top slices
+            ranges.push_back({D - zb, zb - za, k});      // their mirrors in the bottom slab
+        }
+    }
+    int waited[2] = {-1, -1};
+    long long j = 0;
+    for (const Range &r : ranges) {
+        for (long long z = r.z; z < r.z + r.n; z += dz, j++) {
+            const int q = (int)(j & 1);
+            const cudaStream_t st = h->rb[q];
+            if (waited[q] != r.band) {
+                FDK_CUDA(cudaStreamWaitEvent(st, h->band_done[r.band], 0));
+                waited[q] = r.band;
+            }
+            const int n = (int)std::min(dz, r.z + r.n - z);
+            float *buf = h->d_rb + q * plane * dz;
+            const long long tiles = ceil_div((long long)nxs, 32) * ceil_div((long long)n, 32) * nys;
+            const int grid = (int)std::min<long long>(tiles, 148 * 32);
+            if (h->d_comp)
+                transform_volume_kernel<true><<<grid, 32, 0, st>>>(h->d_vol, h->d_comp, buf, nxs, nys, D, z, n);
+            else
+                transform_volume_kernel<false><<<grid, 32, 0, st>>>(h->d_vol, nullptr, buf, nxs, nys, D, z, n);
+            FDK_CUDA(cudaGetLastError());
+            FDK_CUDA(cudaMemcpyAsync(host + plane * z, buf, sizeof(float) * plane * n, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    FDK_CUDA(cudaStreamSynchronize(h->rb[0]));
+    FDK_CUDA(cudaStreamSynchronize(h->rb[1]));
     return FDK_OK;
 }
 
@@ -344,6 +417,41 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             }
         }
     }
+    // z bands: up to kMaxBands launches per batch (FDK_BP_BANDS lowers the cap) when each
+    // still gives every CTA of the persistent grid at least 8 tiles (the split costs nothing
+    // measurable then)
+    h->band_z[0] = 0;
+    h->band_z[1] = (long long)t.depth;
+    if (s == FDK_OK && h->plan.tma_ok && sym) {
+        const int R = precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+        const long long cols = ceil_div((long long)t.width, 16) * ceil_div((long long)t.height, 16);
+        const int tiles_z = (int)ceil_div((long long)t.depth, R);
+        const char *cap = getenv("FDK_BP_BANDS");
+        const int max_bands = cap ? std::max(1, std::min(kMaxBands, atoi(cap))) : kMaxBands;
+        int nb = std::min(max_bands, tiles_z);
+        while (nb > 1 && cols * (tiles_z / nb) < 8ll * h->plan.tma_ctas) nb--;
+        h->n_bands = nb;
+        for (int k = 0; k <= nb; k++) {
+            h->band_tz[k] = (int)((long long)k * tiles_z / nb);
+            h->band_z[k] = std::min<long long>((long long)h->band_tz[k] * R, (long long)t.depth);
+        }
+    }
+    for (int k = 0; k < kMaxBands && s == FDK_OK; k++)
+        ck(cudaEventCreateWithFlags(&h->band_done[k], cudaEventDisableTiming), "event");
+    for (int i = 0; i < 2 && s == FDK_OK; i++)
+        ck(cudaStreamCreateWithFlags(&h->rb[i], cudaStreamNonBlocking), "readback stream");
+    if (s == FDK_OK) {
+        // readback staging: two buffers of whole 32-plane tiles (32 planes, or about 128 MB where
+        // planes are small), allocated here so that a readback never calls the allocator while
+        // the last batch runs
+        const long long plane = (long long)t.width * t.height;
+        const long long want = std::max(32ll, (128ll << 20) / (plane * 4)) / 32 * 32;
+        h->rb_planes = std::max(1ll, std::min(h->D, want));
+        ck(cudaMalloc(&h->d_rb, sizeof(float) * 2 * plane * h->rb_planes), "readback staging");
+    }
+    // the zeroed volume is in place before any readback (those streams do not order after the
+    // default stream)
+    if (s == FDK_OK) ck(cudaDeviceSynchronize(), "create");
     if (s != FDK_OK) {
         fdk_bp_destroy(h);
         return s;
@@ -394,9 +502,11 @@ int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t widt
             to_mirror_half_kernel<<<blocks, 256, 0, h->stream>>>(h->d_stage[k], (__half2 *)h->d_mirror, width, height,
                                                                  n_proj, h->d_absmax, h->plan.d_scale);
             acc_scale = h->plan.d_scale;
+            h->launches += 2;
         } else {
             to_mirror_kernel<float2><<<blocks, 256, 0, h->stream>>>(h->d_stage[k], (float2 *)h->d_mirror, width,
                                                                     height, n_proj);
+            h->launches++;
         }
         FDK_CUDA(cudaGetLastError());
         FDK_TRY(launch_bp(h, h->d_mirror, FDK_LAYOUT_MIRROR, 1, d_mats, proj_mat, n_proj, width, height, h->stream,
@@ -438,12 +548,8 @@ int fdk_bp_get_volume(fdk_bp *h, float *host_vol, int64_t size) {
     FDK_CHECK_ARG(size >= nvox, "size %lld < %lld voxels", (long long)size, nvox);
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_CUDA(cudaStreamSynchronize(h->copy_stream));
-    FDK_CUDA(cudaStreamSynchronize(h->stream));
-    FDK_CUDA(cudaDeviceSynchronize());  // device-resident launches may use caller streams
-    FDK_TRY(check_device_error(h));
-    if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
-    return transform_volume_to_host(h->d_vol, (int)h->top.width, (int)h->top.height, h->D, host_vol, h->stream);
+    FDK_TRY(read_volume(h, host_vol));
+    return check_device_error(h);
     FDK_ABI_END
 }
 
@@ -485,9 +591,11 @@ int fdk_bp_reset(fdk_bp *h) {
     const size_t nvox = (size_t)h->top.width * h->top.height * h->D;
     FDK_CUDA(cudaMemset(h->d_vol, 0, sizeof(float) * nvox));
     if (h->d_comp) FDK_CUDA(cudaMemset(h->d_comp, 0, sizeof(float) * nvox));
+    FDK_CUDA(cudaDeviceSynchronize());  // the readback streams do not order after the default stream
     FDK_TRY(collect_timers(h));
     h->bp_count = 0;
     h->kernel_ms = 0;
+    h->launches = 0;
     return FDK_OK;
     FDK_ABI_END
 }
@@ -517,6 +625,14 @@ int fdk_bp_destroy(fdk_bp *h) {
         if (h->d_mats) cudaFree(h->d_mats);
         if (h->d_absmax) cudaFree(h->d_absmax);
         bp_fast_release(h->plan);
+        for (int k = 0; k < kMaxBands; k++)
+            if (h->band_done[k]) cudaEventDestroy(h->band_done[k]);
+        for (int i = 0; i < 2; i++)
+            if (h->rb[i]) {
+                cudaStreamSynchronize(h->rb[i]);
+                cudaStreamDestroy(h->rb[i]);
+            }
+        if (h->d_rb) cudaFree(h->d_rb);
         if (h->stream) cudaStreamDestroy(h->stream);
         if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     }
@@ -525,6 +641,9 @@ int fdk_bp_destroy(fdk_bp *h) {
 }
 
 }  // extern "C"
+
+// Kernel launches of the handle since creation or the last reset (internal: recon.cu).
+long long fdk_bp_launches_internal(const fdk_bp *h) { return h ? h->launches : 0; }
 
 // Device scalar multiplying the MIXED accumulators of device-resident FP16 views (their
 // producer divided the filtered values by it).  Internal to the library (recon.cu).

@@ -97,6 +97,7 @@ struct BpTmaArgs {
     long long D;
     float wscale;
     int tiles_x, tiles_y, tiles_z;
+    int tz0;  // first z tile of this launch (a launch may cover a band of z tiles)
 };
 
 template <typename E>
@@ -469,7 +470,8 @@ __global__ void __launch_bounds__(288, 2) bp_tma_kernel(const __grid_constant__ 
         int it = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-            const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y, tz = tile / (a.tiles_x * a.tiles_y);
+            const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y;
+            const int tz = a.tz0 + tile / (a.tiles_x * a.tiles_y);
             const float xa = (float)(a.x0 + tx * 16), xb = (float)(a.x0 + min(tx * 16 + 16, a.nxs) - 1);
             const float ya = (float)(a.y0 + ty * 16), yb = (float)(a.y0 + min(ty * 16 + 16, a.nys) - 1);
             const float za = (float)(a.z0 + tz * R), zb = za + (float)(R - 1);
@@ -522,7 +524,8 @@ __global__ void __launch_bounds__(288, 2) bp_tma_kernel(const __grid_constant__ 
     const E *proj = reinterpret_cast<const E *>(a.proj);
     int it = 0;
     for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y, tz = tile / (a.tiles_x * a.tiles_y);
+        const int tx = tile % a.tiles_x, ty = (tile / a.tiles_x) % a.tiles_y;
+        const int tz = a.tz0 + tile / (a.tiles_x * a.tiles_y);
         const int xi = tx * 16 + wx * 8 + lx, yi = ty * 16 + wy * 4 + ly;
         const bool col_ok = xi < a.nxs && yi < a.nys;
         const float x = (float)(a.x0 + xi), y = (float)(a.y0 + yi);
@@ -616,9 +619,12 @@ inline float weight_scale(const float *host_mats, float xc, float yc) {
     return (w > 0.f) ? w * w : 1.0f;
 }
 
+// Backproject n views into the z tiles [tz_begin, tz_end) of R top slices each (with their
+// mirror slices); tz_end < 0 means through the last tile.
 template <typename E>
 inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const void *proj, const float *d_mats,
-                         const float *host_mats, int n, cudaStream_t st, const float *scale) {
+                         const float *host_mats, int n, cudaStream_t st, const float *scale, int tz_begin = 0,
+                         int tz_end = -1) {
     using C = TmaCfg<E>;
     FDK_CHECK_ARG(((uintptr_t)proj & 15) == 0, "TMA views must start on a 16-byte boundary");
     CUtensorMap map;
@@ -643,7 +649,11 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     a.wscale = weight_scale(host_mats, p.x0 + 0.5f * (p.nxs - 1), p.y0 + 0.5f * (p.nys - 1));
     a.tiles_x = (int)ceil_div(p.nxs, 16);
     a.tiles_y = (int)ceil_div(p.nys, 16);
-    a.tiles_z = (int)ceil_div(p.nzz, C::R);
+    const int tz_all = (int)ceil_div(p.nzz, C::R);
+    if (tz_end < 0 || tz_end > tz_all) tz_end = tz_all;
+    FDK_CHECK_ARG(tz_begin >= 0 && tz_begin < tz_end, "z tiles [%d, %d) outside 0..%d", tz_begin, tz_end, tz_all);
+    a.tz0 = tz_begin;
+    a.tiles_z = tz_end - tz_begin;
     const long long n_tiles = (long long)a.tiles_x * a.tiles_y * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, p.tma_ctas);

@@ -55,6 +55,7 @@ struct fdk_recon {
     long long pend_first = 0;
     double filter_ms = 0;
     long long views = 0;
+    long long filter_launches = 0;   // kernel launches of the filter since creation or reset
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ftimers;
     // pinned staging of fdk_recon_push_folder (allocated on first use): two chunks
     float *h_stage[2] = {nullptr, nullptr};
@@ -63,6 +64,7 @@ struct fdk_recon {
 
 // internal hooks (bp.cu)
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
+long long fdk_bp_launches_internal(const fdk_bp *h);
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
                                    int32_t n_proj, const float *host_mats, void *stream);
 
@@ -150,6 +152,7 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
                                  (int)g.nu, h->tables, (int)g.nu, (int)g.nv, h->pad, m, h->layout, h->dtype,
                                  h->compute, h->out_scale, h->d_overflow));
         FDK_CUDA(cudaEventRecord(t.second, h->compute));
+        h->filter_launches += h->tpz ? 2 : 1;  // weighting pass + GEMM, or the fused FFT filter
         h->ftimers.push_back(t);
         h->pending += m;
         done += m;
@@ -424,8 +427,14 @@ int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size) {
     FDK_ABI_BEGIN
     clear_error();
     FDK_CHECK_ARG(h && host_vol, "NULL argument");
-    FDK_TRY(fdk_recon_sync(h, 0));
-    return fdk_bp_get_volume(h->bp, host_vol, size);
+    {
+        DeviceGuard dg(h->device);
+        FDK_TRY(dg.status);
+        FDK_TRY(flush_pending(h));
+    }
+    // band by band, overlapping the last batch's backprojection; then the filter checks
+    FDK_TRY(fdk_bp_get_volume(h->bp, host_vol, size));
+    return fdk_recon_sync(h, 0);
     FDK_ABI_END
 }
 
@@ -445,6 +454,12 @@ int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *vie
     FDK_ABI_END
 }
 
+int fdk_recon_launch_count(fdk_recon *h, int64_t *count) {
+    FDK_CHECK_ARG(h && count, "NULL argument");
+    *count = h->filter_launches + fdk_bp_launches_internal(h->bp);
+    return FDK_OK;
+}
+
 int fdk_recon_reset(fdk_recon *h) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
@@ -456,6 +471,7 @@ int fdk_recon_reset(fdk_recon *h) {
     FDK_CUDA(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)));
     h->filter_ms = 0;
     h->views = 0;
+    h->filter_launches = 0;
     h->pending = 0;  // filtered views not yet backprojected are dropped with the volume
     return fdk_bp_reset(h->bp);
     FDK_ABI_END

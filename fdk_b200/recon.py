@@ -84,6 +84,13 @@ class Reconstructor:
         check(lib().fdk_recon_stats(self._h, C.byref(bp), C.byref(fl), C.byref(n)))
         return {"bp_ms": bp.value, "filter_ms": fl.value, "views": n.value}
 
+    @property
+    def launch_count(self) -> int:
+        """Kernel launches (filter and backprojection) since creation or the last reset."""
+        n = C.c_int64()
+        check(lib().fdk_recon_launch_count(self._h, C.byref(n)))
+        return n.value
+
     def reset(self) -> None:
         check(lib().fdk_recon_reset(self._h))
 

@@ -277,10 +277,13 @@ int fdk_recon_filter_kind(fdk_recon *h, int32_t *kind);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
 /* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).
- * Implies fdk_recon_sync. */
+ * Implies fdk_recon_sync.  Large volumes are backprojected in z bands; each band is copied out
+ * as soon as the last batch has finished it, so most of the copy overlaps that batch. */
 int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size);
 /* Timing: total BP kernel ms, total filter kernel ms, views done. */
 int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views);
+/* Kernel launches (filter and backprojection) since creation or the last reset. */
+int fdk_recon_launch_count(fdk_recon *h, int64_t *count);
 int fdk_recon_reset(fdk_recon *h);
 int fdk_recon_destroy(fdk_recon *h);
 
