@@ -40,7 +40,7 @@ EXPORTED = [
     "fdk_correct_image_real32", "fdk_filter_row_real32", "fdk_filter_row_real32_noalloc",
     "fdk_bp_create", "fdk_bp_bp", "fdk_bp_bp_device", "fdk_bp_get_volume", "fdk_bp_volume_device",
     "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
-    "fdk_rtk_reconstruct_conebeam", "fdk_rtk_backproject_device",
+    "fdk_rtk_reconstruct_conebeam", "fdk_rtk_backproject_device", "fdk_rtk_sync",
     "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device",
     "fdk_recon_push_folder", "fdk_recon_flush", "fdk_recon_filter_kind", "fdk_recon_sync",
     "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_launch_count", "fdk_recon_reset", "fdk_recon_destroy",
@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
         "fdk_bp_destroy": ([vp], C.c_int),
         "fdk_rtk_reconstruct_conebeam": ([vp, vp, vp, vp, vp, vp], C.c_int),
         "fdk_rtk_backproject_device": ([vp, vp, vp, vp, vp, vp, vp], C.c_int),
+        "fdk_rtk_sync": ([vp], C.c_int),
         "fdk_recon_create": ([C.POINTER(vp), G, i32, i32, i32], C.c_int),
         "fdk_recon_create_slab": ([C.POINTER(vp), G, i64, i64, i32, i32, i32], C.c_int),
         "fdk_recon_stream": ([vp, C.POINTER(vp)], C.c_int),

@@ -108,5 +108,10 @@ def rtk_backproject_device(proj_size, vol_size, matrices: np.ndarray, dev_vol_in
     check(lib().fdk_rtk_backproject_device(ps, vs, m.ctypes.data, dev_vol_in, dev_vol_out, dev_proj, stream))
 
 
-__all__ = ["BackProjectionFDK", "BoxT", "reconstruct_conebeam", "rtk_backproject_device", "LAYOUT_MIRROR",
-           "LAYOUT_TRANSPOSED"]
+def rtk_sync(stream: int = 0) -> None:
+    """Wait for stream; raise if the staged RTK kernel reported a device-side failure."""
+    check(lib().fdk_rtk_sync(stream))
+
+
+__all__ = ["BackProjectionFDK", "BoxT", "reconstruct_conebeam", "rtk_backproject_device", "rtk_sync",
+           "LAYOUT_MIRROR", "LAYOUT_TRANSPOSED"]

@@ -236,6 +236,10 @@ int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_s
  * Asynchronous on stream; vol_out may equal vol_in. */
 int fdk_rtk_backproject_device(const int32_t proj_size[3], const int32_t vol_size[3], const float *host_mats,
                                const float *dev_vol_in, float *dev_vol_out, const float *dev_proj, void *stream);
+/* Wait for stream and report (then clear) a device-side failure of the staged RTK kernel: its
+ * bounded pipeline waits ran out (FDK_ERR_DEVICE_CHECK).  fdk_rtk_reconstruct_conebeam checks
+ * this itself; callers of fdk_rtk_backproject_device call it after their launches. */
+int fdk_rtk_sync(void *stream);
 
 /* ---- end-to-end streaming FDK (single-GPU analogue of cuFDK's
  *      FilterThread -> BpThread handoff, cuFDK/mpiFDK.cpp:58-317) ------------- */
