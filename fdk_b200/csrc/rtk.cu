@@ -169,6 +169,7 @@ __device__ __forceinline__ void rtk_view(const float *m, float X, float Y, float
                                          const float *src, int pitch, int u_lo, int v_lo, float wm1, float hm1,
                                          float (&acc)[rtkt::R]) {
     constexpr int R = rtkt::R;
+    const float fk0 = (float)k0;  // one conversion per run; the slices add small exact integers
     if constexpr (ZFREE) {
         const float rw = __fdividef(1.0f, Z);  // fmaf(0, k, Z) == Z
         const float u = X * rw;                 // fmaf(0, k, X) == X
@@ -178,7 +179,7 @@ __device__ __forceinline__ void rtk_view(const float *m, float X, float Y, float
         const float *col = src + ((int)iu - u_lo) - v_lo * pitch;
 #pragma unroll
         for (int kk = 0; kk < R; kk++) {
-            const float fk = (float)(k0 + kk);
+            const float fk = fk0 + (float)kk;  // == (float)(k0 + kk): integers below 2^24
             const float v = fmaf(m[6], fk, Y) * rw;
             float sv = 0.f;
             if (!CHECK || (kk < nk && v >= 0.f && v < hm1)) {
@@ -195,7 +196,7 @@ __device__ __forceinline__ void rtk_view(const float *m, float X, float Y, float
     } else {
 #pragma unroll
         for (int kk = 0; kk < R; kk++) {
-            const float fk = (float)(k0 + kk);
+            const float fk = fk0 + (float)kk;  // == (float)(k0 + kk): integers below 2^24
             const float rw = __fdividef(1.0f, fmaf(m[10], fk, Z));
             const float u = fmaf(m[2], fk, X) * rw, v = fmaf(m[6], fk, Y) * rw;
             float sv = 0.f;
