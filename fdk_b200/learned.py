@@ -132,6 +132,28 @@ class Pipeline:
         self.bp.reset()
         self.bp.BP_device(self.mirror.data_ptr(), LAYOUT_MIRROR, self.mats_h, p.nProj)
 
+    def fov_mask(self):
+        """Voxels whose centre projects inside [0, nu-1) x [0, nv-1) in every view: the fully
+        sampled field of view (a cylinder capped by the cone).  Bool tensor [z][y][x], cached."""
+        if getattr(self, "_fov", None) is None:
+            torch, p = self.torch, self.p
+            z, y, x = torch.meshgrid(*(torch.arange(n, dtype=torch.float64, device=self.dev)
+                                       for n in (p.nz, p.ny, p.nx)), indexing="ij")
+            fov = torch.ones((p.nz, p.ny, p.nx), dtype=torch.bool, device=self.dev)
+            for m in np.asarray(p.proj_matrices(np.float64)).reshape(-1, 12):
+                w = m[8] * x + m[9] * y + m[10] * z + m[11]
+                u = (m[0] * x + m[1] * y + m[2] * z + m[3]) / w
+                v = (m[4] * x + m[5] * y + m[6] * z + m[7]) / w
+                fov &= (w > 0) & (u >= 0) & (u < p.nu - 1) & (v >= 0) & (v < p.nv - 1)
+            self._fov = fov
+        return self._fov
+
+    def mse_fov(self) -> float:
+        """After mse(with_grad=True): the MSE over fov_mask() (the residual holds 2 d / N)."""
+        p = self.p
+        d = self.res * (0.5 * p.nx * p.ny * p.nz)
+        return float((d[self.fov_mask()] ** 2).mean())
+
     def mse(self, with_grad: bool) -> float:
         p = self.p
         vol, _ = self.bp.volume_device()
@@ -201,7 +223,8 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
 
 
 def evaluate(params, n_test: int = 200, seed0: int = 5000, input_window: str | None = None) -> dict:
-    """Held-out scans: MSE of plain FDK, of the learned filter, and of the gated choice."""
+    """Held-out scans: MSE of plain FDK, of the learned filter, and of the gated choice, over the
+    whole volume and over the fully sampled field of view (Pipeline.fov_mask)."""
     import torch
 
     pl = Pipeline(input_window=input_window)
@@ -209,18 +232,24 @@ def evaluate(params, n_test: int = 200, seed0: int = 5000, input_window: str | N
     x = torch.empty((p.nProj, p.nv, p.nu), dtype=torch.float32, device=pl.dev)
     xp = torch.empty_like(x) if pl.engine_in is not pl.engine else x
     w = torch.from_numpy(np.asarray(params, np.float32)).to(pl.dev)
-    plain, learned, kept = [], [], []
+    plain, learned, kept, plain_f, learned_f = [], [], [], [], []
     for i in range(n_test):
         pl.scan(seed0 + i, x, xp if xp is not x else None)
         pl.reconstruct(None, xp)
-        e0 = pl.mse(with_grad=False)
+        e0 = pl.mse(with_grad=True)
+        plain_f.append(pl.mse_fov())
         pl.reconstruct(w, x)
-        e1 = pl.mse(with_grad=False)
+        e1 = pl.mse(with_grad=True)
+        learned_f.append(pl.mse_fov())
         plain.append(e0)
         learned.append(e1)
         kept.append(min(e0, e1))
-    plain, learned, kept = map(np.asarray, (plain, learned, kept))
+    plain, learned, kept, plain_f, learned_f = map(np.asarray, (plain, learned, kept, plain_f, learned_f))
+    kept_f = np.where(learned < plain, learned_f, plain_f)  # the gate decides on the whole volume
     return {"n": n_test, "mse_plain": float(plain.mean()), "mse_learned": float(learned.mean()),
             "mse_kept": float(kept.mean()), "learned_better_frac": float((learned < plain).mean()),
             "mse_reduction": float(1 - kept.mean() / plain.mean()),
-            "rmse_reduction": float(1 - np.sqrt(kept).mean() / np.sqrt(plain).mean())}
+            "rmse_reduction": float(1 - np.sqrt(kept).mean() / np.sqrt(plain).mean()),
+            "fov_fraction": float(pl.fov_mask().float().mean()),
+            "fov_mse_plain": float(plain_f.mean()), "fov_mse_kept": float(kept_f.mean()),
+            "fov_mse_reduction": float(1 - kept_f.mean() / plain_f.mean())}

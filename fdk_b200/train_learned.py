@@ -2,6 +2,7 @@
 
     python -m fdk_b200.train_learned [--n-train 2000] [--epochs 20] [--n-test 200]
                                       [--time-limit S] [--out fdk_b200/weights/residual_c5.npz]
+    python -m fdk_b200.train_learned --eval-only [--out weights.npz]   # held-out result only
 
 Writes the trained parameters (npz) and prints one JSON line with the held-out result: MSE of
 plain Hann-ramp FDK, of the learned filter, and of the gated choice (the learned reconstruction
@@ -31,6 +32,7 @@ def main():
     ap.add_argument("--time-limit", type=float, default=None, help="stop training after this many seconds")
     ap.add_argument("--schedule", default="cosine", choices=["constant", "cosine"])
     ap.add_argument("--input-window", default=None, help="ramp window of the network's input rows (default: hann)")
+    ap.add_argument("--eval-only", action="store_true", help="evaluate the weights at --out, no training")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                   "residual_c5.npz"))
     args = ap.parse_args()
@@ -39,6 +41,12 @@ def main():
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
 
     window = args.input_window or "hann"
+    if args.eval_only:
+        w = np.load(args.out)
+        window = str(w["input_window"]) if "input_window" in w else window
+        ev = learned.evaluate(w["params"], args.n_test, input_window=None if window == "hann" else window)
+        print(json.dumps({"weights": os.path.relpath(args.out), "input_window": window, "eval": ev}), flush=True)
+        return
 
     def checkpoint(ep, params, hist):
         np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * args.n_train,
