@@ -48,7 +48,7 @@ struct fdk_recon {
     float *d_mats = nullptr;         // the same on the device
     cudaStream_t compute = nullptr, copy = nullptr;
     std::vector<cudaEvent_t> raw_ready, raw_free;
-    cudaEvent_t f0 = nullptr, f1 = nullptr, done = nullptr;
+    cudaEvent_t done = nullptr;
     int slot = 0;
     // filtered views waiting in d_filt for a full batch: views pend_first .. pend_first+pending-1
     int pending = 0;
@@ -117,7 +117,8 @@ int collect_filter_timers(fdk_recon *h) {
     return FDK_OK;
 }
 
-// Backproject the filtered views waiting in d_filt (one launch), on the compute stream.
+// Backproject the filtered views waiting in d_filt (one batch: a launch per z band), on the
+// compute stream.
 int flush_pending(fdk_recon *h) {
     if (h->pending == 0) return FDK_OK;
     FDK_TRY(fdk_bp_bp_device_mats_internal(h->bp, h->d_filt, h->layout, h->d_mats + 12 * h->pend_first, h->pending,
@@ -250,7 +251,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         if (s == FDK_OK) ck(cudaMemcpy(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice), "scale");
         // the filter, chosen by measurement: on the C3/C4 workloads the split-FP16 tensor-core
         // GEMM (fdk_toeplitz_*) matches the FFT filter's accuracy (rel-L2 2e-4, the FP16 output
-        // rounding) in 0.46x (C3) / 0.65x (C4) of its time.  The FFT filter remains where the GEMM
+        // rounding) in 0.29x (C3) / 0.37x (C4) of its time.  The FFT filter remains where the GEMM
         // cannot run (nu not a multiple of 256, nv of 128) or when FDK_FILTER=fft.
         const char *want = std::getenv("FDK_FILTER");
         const bool fft_only = want && std::string(want) == "fft";
