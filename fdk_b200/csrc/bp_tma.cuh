@@ -42,7 +42,10 @@ struct TmaCfg;
 // workload, 128 views per launch: mixed R 12 -> 16 and 4 -> 8 views per stage 1985 -> 2215 GUPS
 // (more stages changed nothing; R >= 20 spills); FP32 R 8 -> 12: 1007 -> 1051 GUPS.  Unrolling
 // the view loop (1641 GUPS) and pairing two views per slice with an FP16 pre-add (2115 GUPS)
-// were slower: both raise register pressure past the 2-CTA budget.
+// were slower: both raise register pressure past the 2-CTA budget.  Three CTAs per SM (72
+// registers; FDK_TMA_MIN_BLOCKS=3) were slower too: R 12 with 4 or 6 views per stage 2003 /
+// 1960 GUPS, R 8 with 4 views 1830 GUPS -- the per-column setup amortised over fewer slices costs
+// more than the extra warps gain.
 #ifndef FDK_TMA_MIXED_R
 #define FDK_TMA_MIXED_R 16
 #endif
@@ -394,7 +397,10 @@ __device__ __forceinline__ void write_back(float *__restrict__ vol, float *__res
 }
 
 template <typename E>
-__global__ void __launch_bounds__(288, 2) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
+#ifndef FDK_TMA_MIN_BLOCKS
+#define FDK_TMA_MIN_BLOCKS 2
+#endif
+__global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
     using C = TmaCfg<E>;
     constexpr int R = C::R, NV = C::NV, S = C::S;
     constexpr int BOX = tma_box_bytes<E>();
