@@ -10,7 +10,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("nu,nv,views,dtype,split", [(256, 128, 3, "f16", False), (512, 256, 2, "f16", True),
-                                                     (1536, 128, 1, "f16", True), (512, 128, 2, "bf16", False),
+                                                     (1536, 128, 1, "f16", True), (2048, 128, 1, "f16", True),
+                                                     (512, 128, 2, "bf16", False),
                                                      (512, 128, 1, "bf16", True)])
 def test_toeplitz_gemm_vs_oracle(nu, nv, views, dtype, split):
     import torch
