@@ -174,8 +174,9 @@ class Pipeline:
 
 def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 1000, params=None, log=print,
           time_limit_s: float | None = None, on_epoch=None, schedule: str = "constant",
-          input_window: str | None = None) -> dict:
-    """Adam on volume MSE, one phantom per step; the training scans are generated once.
+          input_window: str | None = None, batch: int = 1) -> dict:
+    """Adam on volume MSE; the training scans are generated once.  batch: phantoms per Adam
+    step (their gradients averaged; 1 = one phantom per step).
     schedule: "constant" (lr throughout) or "cosine" (lr decayed to lr/100 over all steps).
     on_epoch(epoch, params, history), when given, runs after every epoch (checkpointing)."""
     import torch
@@ -191,19 +192,28 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
     w = torch.from_numpy(init_params() if params is None else np.asarray(params, np.float32)).to(pl.dev)
     m = torch.zeros_like(w)
     v = torch.zeros_like(w)
+    gsum = torch.zeros_like(w)
     hist, step, t0 = [], 0, time.time()
-    total = n_train * epochs
+    total = max(1, (n_train // batch) * epochs)
     rng = np.random.default_rng(7)
     stopped = False
     for ep in range(epochs):
         order = rng.permutation(n_train)
         tot = 0.0
-        for i in order:
-            pl.truth_of(seed0 + int(i))
-            pl.reconstruct(w, xs[i])
-            tot += pl.mse(with_grad=True)
-            pl.gradient(w, xs[i])
+        n_done = 0
+        for b0 in range(0, n_train - batch + 1, batch):
+            for i in order[b0:b0 + batch]:
+                pl.truth_of(seed0 + int(i))
+                pl.reconstruct(w, xs[i])
+                tot += pl.mse(with_grad=True)
+                pl.gradient(w, xs[i])
+                if batch > 1:
+                    gsum += pl.dparams
+            n_done += batch
             step += 1
+            if batch > 1:
+                torch.mul(gsum, 1.0 / batch, out=pl.dparams)
+                gsum.zero_()
             lr_t = lr if schedule == "constant" else lr * (0.01 + 0.99 * 0.5 * (1 + math.cos(math.pi * step / total)))
             check(lib().fdk_adam_step(w.data_ptr(), pl.dparams.data_ptr(), m.data_ptr(), v.data_ptr(), w.numel(),
                                       lr_t, 0.9, 0.999, 1e-8, step, None))
@@ -211,7 +221,6 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
                 stopped = True
                 break
         torch.cuda.synchronize()
-        n_done = len(order) if not stopped else (step - ep * n_train)
         hist.append(tot / max(1, n_done))
         log(f"epoch {ep}: train MSE {hist[-1]:.4e} ({time.time() - t0:.0f} s, {step} steps)")
         if on_epoch is not None:

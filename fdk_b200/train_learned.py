@@ -32,6 +32,7 @@ def main():
     ap.add_argument("--time-limit", type=float, default=None, help="stop training after this many seconds")
     ap.add_argument("--schedule", default="cosine", choices=["constant", "cosine"])
     ap.add_argument("--input-window", default=None, help="ramp window of the network's input rows (default: hann)")
+    ap.add_argument("--batch", type=int, default=1, help="phantoms per Adam step (gradients averaged)")
     ap.add_argument("--eval-only", action="store_true", help="evaluate the weights at --out, no training")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                   "residual_c5.npz"))
@@ -49,15 +50,15 @@ def main():
         return
 
     def checkpoint(ep, params, hist):
-        np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * args.n_train,
+        np.savez(args.out, params=params, history=np.asarray(hist), steps=(ep + 1) * (args.n_train // args.batch),
                  input_window=window)
 
     tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit, on_epoch=checkpoint,
-                       schedule=args.schedule, input_window=args.input_window)
+                       schedule=args.schedule, input_window=args.input_window, batch=args.batch)
     np.savez(args.out, params=tr["params"], history=np.asarray(tr["history"]), steps=tr["steps"], input_window=window)
     ev = learned.evaluate(tr["params"], args.n_test, input_window=args.input_window)
     out = {"workload": "C5: 256^3, 90 views of 256^2, I0=1e4, mu=0.02/mm", "n_train": args.n_train,
-           "schedule": args.schedule, "input_window": window, "lr": args.lr,
+           "schedule": args.schedule, "input_window": window, "lr": args.lr, "batch": args.batch,
            "epochs_requested": args.epochs, "epochs_run": len(tr["history"]), "steps": tr["steps"],
            "stopped_early": tr["stopped_early"], "train_seconds": tr["seconds"], "history": tr["history"],
            "eval": ev, "total_seconds": time.time() - t0, "weights": os.path.relpath(args.out)}
