@@ -14,7 +14,7 @@
 // adjacent index bits, so the 8 elements that differ only in those bits form a closed group.
 // Every butterfly is the plain radix-2 one, so the arithmetic is that of the stage-by-stage
 // transform, with a third of the shared-memory round trips and barriers.  Twiddles come from
-// an FP64-computed table.
+// an FP64-computed table, rearranged per pass so that a group reads its own with vector loads.
 //
 // The backprojection's MIRROR layout is written by filter_mirror_kernel: a CTA filters G row
 // pairs in turn, collects their outputs as an nu x G tile per side in shared memory, and writes
@@ -36,6 +36,7 @@ struct FilterArgs {
     void *dst;          // output, layout dependent
     const float *cos;   // nv x nu (pitch cos_pitch) or nullptr
     const float2 *tw;   // W/2 twiddles exp(-2 pi i k / W)
+    const float2 *twp;  // per pass and group, the group's twiddles (FilterTables::twp) or nullptr
     const float *hb;    // W: H[bitrev(p)] / W
     int nu, nv, W, log2W, off, pad_n;
     int src_pitch, dst_pitch, cos_pitch;
@@ -69,34 +70,65 @@ __device__ __forceinline__ float row_sample(const FilterArgs &a, const float *vi
     return x;
 }
 
+// Shared-memory position of element i of an FFT: i ^ ((i >> 4) & 15), a permutation inside each
+// block of 16 float2.  Later DIF and early DIT passes read groups 8 or 64 elements apart, which
+// in the plain layout fall into the same banks (up to 16-way conflicts); the swizzle spreads
+// them, and contiguous runs stay contiguous within their block (about 2.5 wavefronts per warp
+// access against 6 for the plain layout, in a model of the passes at W = 512 .. 4096).
+__device__ __forceinline__ int fsw(int i) { return i ^ ((i >> 4) & 15); }
+
+// Twiddles of a group.  A DIF pass starting at stage s0 needs, for stage t and butterfly j,
+// tw[(g_low + (j mod 2^(NS-1-t)) 2^low) << (s0 + t)], and a DIT pass starting at bit b0
+// tw[(g_low + (j mod 2^t) 2^b0) << (log2W - 1 - b0 - t)] (g_low: the group's index bits below
+// the pass): 2^NS - 1 distinct values, listed stage by stage.  FilterTables keeps them per pass
+// and group, padded to 2^NS entries, so a thread reads its group's list with 16-byte loads and
+// neighbouring groups' lists are adjacent; without that table (twp == nullptr) the list is
+// gathered from tw.  (One scattered load per butterfly made the kernel L1-bound.)
+
 // One pass of NS consecutive radix-2 DIF stages, the first being stage s0 (half = W >> (s0+1)).
 // Those stages touch index bits hbit .. hbit-NS+1; a group is the 2^NS elements that differ only
 // there.  Butterfly: (x, y) -> (x + y, (x - y) tw[(i & (half-1)) << stage]).  hb_tab (last pass
-// only) multiplies the bit-reversed result by H[bitrev(p)] / W.
+// only) multiplies the bit-reversed result by H[bitrev(p)] / W.  twp: this pass's group lists.
 template <int NS>
-__device__ __forceinline__ void dif_pass(float2 *buf0, const float2 *__restrict__ tw, const float *__restrict__ hb_tab,
-                                         int W, int log2W, int s0, int count) {
+__device__ __forceinline__ void dif_pass(float2 *buf0, const float2 *__restrict__ tw, const float2 *__restrict__ twp,
+                                         const float *__restrict__ hb_tab, int W, int log2W, int s0, int count) {
     constexpr int GS = 1 << NS;
     const int hbit = log2W - 1 - s0;
     const int low = hbit - NS + 1;
     for (int gg = threadIdx.x; gg < (count << (log2W - NS)); gg += blockDim.x) {
         float2 *buf = buf0 + ((gg >> (log2W - NS)) << log2W);  // FFT gg / (W >> NS) of count
         const int g = gg & ((W >> NS) - 1);
-        const int base = ((g >> low) << (hbit + 1)) | (g & ((1 << low) - 1));
+        const int g_low = g & ((1 << low) - 1);
+        const int base = ((g >> low) << (hbit + 1)) | g_low;
         float2 v[GS];
 #pragma unroll
-        for (int j = 0; j < GS; j++) v[j] = buf[base + (j << low)];
+        for (int j = 0; j < GS; j++) v[j] = buf[fsw(base + (j << low))];
+        float2 tq[GS];  // stage t's list starts at GS - (GS >> t)
+        if (twp) {
+            const float4 *q = reinterpret_cast<const float4 *>(twp + g_low * GS);
+#pragma unroll
+            for (int k = 0; k < GS / 2; k++) {
+                const float4 f = __ldg(q + k);
+                tq[2 * k] = make_float2(f.x, f.y);
+                tq[2 * k + 1] = make_float2(f.z, f.w);
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < NS; t++)
+#pragma unroll
+                for (int jt = 0; jt < (GS >> (t + 1)); jt++)
+                    tq[GS - (GS >> t) + jt] = __ldg(tw + ((g_low + (jt << low)) << (s0 + t)));
+        }
 #pragma unroll
         for (int t = 0; t < NS; t++) {
             const int hstep = GS >> (t + 1);
-            const int half = 1 << (hbit - t);
 #pragma unroll
             for (int j = 0; j < GS; j++) {
                 if (j & hstep) continue;
-                const int i0 = base + (j << low);
+                const float2 w = tq[GS - (GS >> t) + (j & ((1 << (NS - 1 - t)) - 1))];
                 const float2 x = v[j], y = v[j + hstep];
                 v[j] = make_float2(x.x + y.x, x.y + y.y);
-                v[j + hstep] = cmul(make_float2(x.x - y.x, x.y - y.y), __ldg(tw + ((i0 & (half - 1)) << (s0 + t))));
+                v[j + hstep] = cmul(make_float2(x.x - y.x, x.y - y.y), w);
             }
         }
         if (hb_tab) {
@@ -107,58 +139,76 @@ __device__ __forceinline__ void dif_pass(float2 *buf0, const float2 *__restrict_
             }
         }
 #pragma unroll
-        for (int j = 0; j < GS; j++) buf[base + (j << low)] = v[j];
+        for (int j = 0; j < GS; j++) buf[fsw(base + (j << low))] = v[j];
     }
 }
-
-// One pass of NS consecutive radix-2 DIT stages on index bits b0 .. b0+NS-1 (half = 2^b0 first).
-// Butterfly: t = y conj(tw[(i & (half-1)) * W / (2 half)]); (x, y) -> (x + t, x - t).
 template <int NS>
-__device__ __forceinline__ void dit_pass(float2 *buf0, const float2 *__restrict__ tw, int W, int log2W, int b0,
-                                         int count) {
+__device__ __forceinline__ void dit_pass(float2 *buf0, const float2 *__restrict__ tw, const float2 *__restrict__ twp,
+                                         int W, int log2W, int b0, int count) {
     constexpr int GS = 1 << NS;
     for (int gg = threadIdx.x; gg < (count << (log2W - NS)); gg += blockDim.x) {
         float2 *buf = buf0 + ((gg >> (log2W - NS)) << log2W);
         const int g = gg & ((W >> NS) - 1);
-        const int base = ((g >> b0) << (b0 + NS)) | (g & ((1 << b0) - 1));
+        const int g_low = g & ((1 << b0) - 1);
+        const int base = ((g >> b0) << (b0 + NS)) | g_low;
         float2 v[GS];
 #pragma unroll
-        for (int j = 0; j < GS; j++) v[j] = buf[base + (j << b0)];
+        for (int j = 0; j < GS; j++) v[j] = buf[fsw(base + (j << b0))];
+        float2 tq[GS];  // stage t's list starts at 2^t - 1
+        if (twp) {
+            const float4 *q = reinterpret_cast<const float4 *>(twp + g_low * GS);
+#pragma unroll
+            for (int k = 0; k < GS / 2; k++) {
+                const float4 f = __ldg(q + k);
+                tq[2 * k] = make_float2(f.x, f.y);
+                tq[2 * k + 1] = make_float2(f.z, f.w);
+            }
+        } else {
+#pragma unroll
+            for (int t = 0; t < NS; t++)
+#pragma unroll
+                for (int jt = 0; jt < (1 << t); jt++)
+                    tq[(1 << t) - 1 + jt] = __ldg(tw + ((g_low + (jt << b0)) << (log2W - 1 - b0 - t)));
+        }
 #pragma unroll
         for (int t = 0; t < NS; t++) {
             const int hstep = 1 << t;
-            const int half = 1 << (b0 + t);
 #pragma unroll
             for (int j = 0; j < GS; j++) {
                 if (j & hstep) continue;
-                const int i0 = base + (j << b0);
+                const float2 w = tq[(1 << t) - 1 + (j & ((1 << t) - 1))];
                 const float2 x = v[j];
-                const float2 u = cmulc(v[j + hstep], __ldg(tw + ((i0 & (half - 1)) << (log2W - 1 - b0 - t))));
+                const float2 u = cmulc(v[j + hstep], w);
                 v[j] = make_float2(x.x + u.x, x.y + u.y);
                 v[j + hstep] = make_float2(x.x - u.x, x.y - u.y);
             }
         }
 #pragma unroll
-        for (int j = 0; j < GS; j++) buf[base + (j << b0)] = v[j];
+        for (int j = 0; j < GS; j++) buf[fsw(base + (j << b0))] = v[j];
     }
 }
 
 // Forward transform, multiply by H, inverse transform of `count` W-point FFTs stored one after
 // the other in buf; ends after a barrier.
 __device__ __forceinline__ void filter_fft(float2 *buf, const FilterArgs &a, int count = 1) {
+    long long off = 0;  // this pass's group lists in a.twp: the DIF passes', then the DIT passes'
     for (int s = 0; s < a.log2W; s += 3) {
         const int ns = min(3, a.log2W - s);
         const float *h = (s + ns == a.log2W) ? a.hb : nullptr;
-        if (ns == 3) dif_pass<3>(buf, a.tw, h, a.W, a.log2W, s, count);
-        else if (ns == 2) dif_pass<2>(buf, a.tw, h, a.W, a.log2W, s, count);
-        else dif_pass<1>(buf, a.tw, h, a.W, a.log2W, s, count);
+        const float2 *twp = a.twp ? a.twp + off : nullptr;
+        if (ns == 3) dif_pass<3>(buf, a.tw, twp, h, a.W, a.log2W, s, count);
+        else if (ns == 2) dif_pass<2>(buf, a.tw, twp, h, a.W, a.log2W, s, count);
+        else dif_pass<1>(buf, a.tw, twp, h, a.W, a.log2W, s, count);
+        off += (long long)(1 << ns) << (a.log2W - s - ns);
         __syncthreads();
     }
     for (int b = 0; b < a.log2W; b += 3) {
         const int ns = min(3, a.log2W - b);
-        if (ns == 3) dit_pass<3>(buf, a.tw, a.W, a.log2W, b, count);
-        else if (ns == 2) dit_pass<2>(buf, a.tw, a.W, a.log2W, b, count);
-        else dit_pass<1>(buf, a.tw, a.W, a.log2W, b, count);
+        const float2 *twp = a.twp ? a.twp + off : nullptr;
+        if (ns == 3) dit_pass<3>(buf, a.tw, twp, a.W, a.log2W, b, count);
+        else if (ns == 2) dit_pass<2>(buf, a.tw, twp, a.W, a.log2W, b, count);
+        else dit_pass<1>(buf, a.tw, twp, a.W, a.log2W, b, count);
+        off += (long long)(1 << ns) << b;
         __syncthreads();
     }
 }
@@ -197,7 +247,7 @@ __global__ void __launch_bounds__(256) filter_rows_kernel(FilterArgs a) {
             x1 = row_sample(a, vsrc, r1, c);
             x2 = row_sample(a, vsrc, r2, c);
         }
-        buf[k] = make_float2(x1, x2);
+        buf[fsw(k)] = make_float2(x1, x2);
     }
     __syncthreads();
 
@@ -205,7 +255,7 @@ __global__ void __launch_bounds__(256) filter_rows_kernel(FilterArgs a) {
 
     OUT *dst = reinterpret_cast<OUT *>(a.dst);
     for (int u = threadIdx.x; u < a.nu; u += blockDim.x) {
-        const float2 y = buf[a.off + u];
+        const float2 y = buf[fsw(a.off + u)];
         const OUT o1 = to_out<OUT>(a, y.x), o2 = to_out<OUT>(a, y.y);
         if (LAYOUT == FDK_LAYOUT_ROWS) {
             OUT *d = dst + (long long)view * a.dst_vstride;
@@ -244,7 +294,7 @@ struct PairOf<__half> {
 // NP = min(G, 4096 / W) pairs are transformed at once, so every 3-stage pass keeps all 512
 // threads busy (W / 8 groups per FFT).
 template <typename OUT, int G>
-__global__ void __launch_bounds__(512) filter_mirror_kernel(FilterArgs a) {
+__global__ void __launch_bounds__(512, 2) filter_mirror_kernel(FilterArgs a) {
     using P = typename PairOf<OUT>::T;
     static_assert(G * sizeof(P) == 16, "one 16-byte store per column and side");
     extern __shared__ __align__(16) unsigned char fsm[];
@@ -274,13 +324,13 @@ __global__ void __launch_bounds__(512) filter_mirror_kernel(FilterArgs a) {
                 x1 = row_sample(a, vsrc, r1, c);
                 x2 = row_sample(a, vsrc, r2, c);
             }
-            buf[k] = make_float2(x1, x2);
+            buf[(q << a.log2W) + fsw(k & (a.W - 1))] = make_float2(x1, x2);
         }
         __syncthreads();
         filter_fft(buf, a, NP);
         for (int k = threadIdx.x; k < NP * a.nu; k += blockDim.x) {
             const int q = k / a.nu, u = k - q * a.nu, g = g0 + q;
-            const float2 y = buf[(q << a.log2W) + a.off + u];
+            const float2 y = buf[(q << a.log2W) + fsw(a.off + u)];
             const OUT o1 = to_out<OUT>(a, y.x), o2 = to_out<OUT>(a, y.y);
             stg[u * G + g] = PairOf<OUT>::make(o1, o2);                     // element (u, r1)
             stg[(a.nu + u) * G + (G - 1 - g)] = PairOf<OUT>::make(o2, o1);  // element (u, r2)
@@ -312,17 +362,42 @@ int FilterTables::create(const double *H, int W_) {
             if (p & (1 << b)) r |= 1 << (log2W - 1 - b);
         h[p] = (float)(H[r] / W);
     }
+    // the group lists of every pass, in filter_fft's order (DIF passes, then DIT passes); each
+    // group's list padded to 2^ns entries
+    std::vector<float2> pt;
+    for (int s0 = 0; s0 < log2W; s0 += 3) {
+        const int ns = std::min(3, log2W - s0), GS = 1 << ns, low = log2W - s0 - ns;
+        for (int g = 0; g < (1 << low); g++) {
+            const size_t at = pt.size();
+            for (int st = 0; st < ns; st++)
+                for (int jt = 0; jt < (GS >> (st + 1)); jt++) pt.push_back(t[(g + (jt << low)) << (s0 + st)]);
+            pt.resize(at + GS, make_float2(0.f, 0.f));
+        }
+    }
+    for (int b0 = 0; b0 < log2W; b0 += 3) {
+        const int ns = std::min(3, log2W - b0), GS = 1 << ns;
+        for (int g = 0; g < (1 << b0); g++) {
+            const size_t at = pt.size();
+            for (int st = 0; st < ns; st++)
+                for (int jt = 0; jt < (1 << st); jt++) pt.push_back(t[(g + (jt << b0)) << (log2W - 1 - b0 - st)]);
+            pt.resize(at + GS, make_float2(0.f, 0.f));
+        }
+    }
     FDK_CUDA(cudaMalloc(&tw, sizeof(float2) * (W / 2)));
     FDK_CUDA(cudaMalloc(&hb, sizeof(float) * W));
+    FDK_CUDA(cudaMalloc(&twp, sizeof(float2) * pt.size()));
     FDK_CUDA(cudaMemcpy(tw, t.data(), sizeof(float2) * (W / 2), cudaMemcpyHostToDevice));
     FDK_CUDA(cudaMemcpy(hb, h.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
+    FDK_CUDA(cudaMemcpy(twp, pt.data(), sizeof(float2) * pt.size(), cudaMemcpyHostToDevice));
     return FDK_OK;
 }
 
 void FilterTables::release() {
     if (tw) cudaFree(tw);
+    if (twp) cudaFree(twp);
     if (hb) cudaFree(hb);
     tw = nullptr;
+    twp = nullptr;
     hb = nullptr;
 }
 
@@ -388,6 +463,7 @@ int filter_views(const float *src, int src_pitch, long long src_vstride, void *d
     a.dst = dst;
     a.cos = cos;
     a.tw = t.tw;
+    a.twp = t.twp;
     a.hb = t.hb;
     a.nu = nu;
     a.nv = nv;

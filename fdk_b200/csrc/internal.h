@@ -13,6 +13,7 @@ void projection_matrix(const fdk_geometry &g, double a, double *m);
 struct FilterTables {
     int W = 0, log2W = 0;
     float2 *tw = nullptr;
+    float2 *twp = nullptr;  // per FFT pass and group, the group's twiddles (optional)
     float *hb = nullptr;
     int create(const double *H, int W_);
     void release();
