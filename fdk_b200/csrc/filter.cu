@@ -80,10 +80,11 @@ __device__ __forceinline__ int fsw(int i) { return i ^ ((i >> 4) & 15); }
 // Twiddles of a group.  A DIF pass starting at stage s0 needs, for stage t and butterfly j,
 // tw[(g_low + (j mod 2^(NS-1-t)) 2^low) << (s0 + t)], and a DIT pass starting at bit b0
 // tw[(g_low + (j mod 2^t) 2^b0) << (log2W - 1 - b0 - t)] (g_low: the group's index bits below
-// the pass): 2^NS - 1 distinct values, listed stage by stage.  FilterTables keeps them per pass
-// and group, padded to 2^NS entries, so a thread reads its group's list with 16-byte loads and
-// neighbouring groups' lists are adjacent; without that table (twp == nullptr) the list is
-// gathered from tw.  (One scattered load per butterfly made the kernel L1-bound.)
+// the pass): 2^NS - 1 distinct values, listed stage by stage and padded to 2^NS.  FilterTables
+// keeps every pass's lists as 2^(NS-1) planes of 16-byte pairs, plane k holding pair k of every
+// group in group order, so a warp's k-th load covers consecutive 16-byte words; without that
+// table (twp == nullptr) the list is gathered from tw.  (One scattered load per butterfly made
+// the kernel L1-bound.)
 
 // One pass of NS consecutive radix-2 DIF stages, the first being stage s0 (half = W >> (s0+1)).
 // Those stages touch index bits hbit .. hbit-NS+1; a group is the 2^NS elements that differ only
@@ -105,10 +106,10 @@ __device__ __forceinline__ void dif_pass(float2 *buf0, const float2 *__restrict_
         for (int j = 0; j < GS; j++) v[j] = buf[fsw(base + (j << low))];
         float2 tq[GS];  // stage t's list starts at GS - (GS >> t)
         if (twp) {
-            const float4 *q = reinterpret_cast<const float4 *>(twp + g_low * GS);
+            const float4 *q = reinterpret_cast<const float4 *>(twp) + g_low;
 #pragma unroll
             for (int k = 0; k < GS / 2; k++) {
-                const float4 f = __ldg(q + k);
+                const float4 f = __ldg(q + (k << low));  // plane k of 2^low groups
                 tq[2 * k] = make_float2(f.x, f.y);
                 tq[2 * k + 1] = make_float2(f.z, f.w);
             }
@@ -156,10 +157,10 @@ __device__ __forceinline__ void dit_pass(float2 *buf0, const float2 *__restrict_
         for (int j = 0; j < GS; j++) v[j] = buf[fsw(base + (j << b0))];
         float2 tq[GS];  // stage t's list starts at 2^t - 1
         if (twp) {
-            const float4 *q = reinterpret_cast<const float4 *>(twp + g_low * GS);
+            const float4 *q = reinterpret_cast<const float4 *>(twp) + g_low;
 #pragma unroll
             for (int k = 0; k < GS / 2; k++) {
-                const float4 f = __ldg(q + k);
+                const float4 f = __ldg(q + (k << b0));  // plane k of 2^b0 groups
                 tq[2 * k] = make_float2(f.x, f.y);
                 tq[2 * k + 1] = make_float2(f.z, f.w);
             }
@@ -363,25 +364,37 @@ int FilterTables::create(const double *H, int W_) {
         h[p] = (float)(H[r] / W);
     }
     // the group lists of every pass, in filter_fft's order (DIF passes, then DIT passes); each
-    // group's list padded to 2^ns entries
+    // group's list padded to 2^ns entries and stored as 2^(ns-1) planes of pairs (pair k of
+    // group g at (k * groups + g) * 2)
     std::vector<float2> pt;
+    auto put_pass = [&](int groups, int GS, const std::vector<float2> &lists) {  // lists: groups x GS
+        for (int k = 0; k < GS / 2; k++)
+            for (int g = 0; g < groups; g++) {
+                pt.push_back(lists[(size_t)g * GS + 2 * k]);
+                pt.push_back(lists[(size_t)g * GS + 2 * k + 1]);
+            }
+    };
     for (int s0 = 0; s0 < log2W; s0 += 3) {
         const int ns = std::min(3, log2W - s0), GS = 1 << ns, low = log2W - s0 - ns;
+        std::vector<float2> lists((size_t)GS << low, make_float2(0.f, 0.f));
         for (int g = 0; g < (1 << low); g++) {
-            const size_t at = pt.size();
+            int e = 0;
             for (int st = 0; st < ns; st++)
-                for (int jt = 0; jt < (GS >> (st + 1)); jt++) pt.push_back(t[(g + (jt << low)) << (s0 + st)]);
-            pt.resize(at + GS, make_float2(0.f, 0.f));
+                for (int jt = 0; jt < (GS >> (st + 1)); jt++)
+                    lists[(size_t)g * GS + e++] = t[(g + (jt << low)) << (s0 + st)];
         }
+        put_pass(1 << low, GS, lists);
     }
     for (int b0 = 0; b0 < log2W; b0 += 3) {
         const int ns = std::min(3, log2W - b0), GS = 1 << ns;
+        std::vector<float2> lists((size_t)GS << b0, make_float2(0.f, 0.f));
         for (int g = 0; g < (1 << b0); g++) {
-            const size_t at = pt.size();
+            int e = 0;
             for (int st = 0; st < ns; st++)
-                for (int jt = 0; jt < (1 << st); jt++) pt.push_back(t[(g + (jt << b0)) << (log2W - 1 - b0 - st)]);
-            pt.resize(at + GS, make_float2(0.f, 0.f));
+                for (int jt = 0; jt < (1 << st); jt++)
+                    lists[(size_t)g * GS + e++] = t[(g + (jt << b0)) << (log2W - 1 - b0 - st)];
         }
+        put_pass(1 << b0, GS, lists);
     }
     FDK_CUDA(cudaMalloc(&tw, sizeof(float2) * (W / 2)));
     FDK_CUDA(cudaMalloc(&hb, sizeof(float) * W));
