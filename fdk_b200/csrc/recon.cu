@@ -251,7 +251,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         if (s == FDK_OK) ck(cudaMemcpy(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice), "scale");
         // the filter, chosen by measurement: on the C3/C4 workloads the split-FP16 tensor-core
         // GEMM (fdk_toeplitz_*) matches the FFT filter's accuracy (rel-L2 2e-4, the FP16 output
-        // rounding) in 0.29x (C3) / 0.37x (C4) of its time.  The FFT filter remains where the GEMM
+        // rounding) in 0.61x (C3) / 0.67x (C4) of its time.  The FFT filter remains where the GEMM
         // cannot run (nu not a multiple of 256, nv of 128) or when FDK_FILTER=fft.
         const char *want = std::getenv("FDK_FILTER");
         const bool fft_only = want && std::string(want) == "fft";
