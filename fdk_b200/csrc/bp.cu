@@ -136,7 +136,13 @@ __global__ void transpose_views_kernel(const float *__restrict__ src, float *__r
 using namespace fdk;
 
 namespace {
-constexpr int kMaxBands = 4;
+// Most z bands per batch (tuning macro).  On the 2048^3 workload 8 bands measured the same as 4
+// (e2e 2203 against 2205 GUPS on one box): the readback then trails the PCIe copy, not the
+// first band.
+#ifndef FDK_MAX_BANDS
+#define FDK_MAX_BANDS 4
+#endif
+constexpr int kMaxBands = FDK_MAX_BANDS;
 }
 
 struct fdk_bp {
