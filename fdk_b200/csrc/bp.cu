@@ -210,9 +210,13 @@ int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
 // Backproject n views already resident on the device.
 //   layout TRANSPOSED: f32 frames of proj_h rows x proj_w (the reference's BP input)
 //   layout MIRROR: mirror pairs (f32x2 or f16x2 per precision), proj_h rows x proj_w pairs
+//   band: -1 = every z band (the whole volume), else that band only (views counted with band 0;
+//   kernels without bands run whole with band 0 and do nothing for the others)
 int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const float *d_mats,
               const float *host_mats, int n, int width, int height, cudaStream_t st,
-              const float *acc_scale = nullptr) {
+              const float *acc_scale = nullptr, int band = -1) {
+    FDK_CHECK_ARG(band < h->n_bands, "band %d outside 0..%d", band, h->n_bands - 1);
+    const int kb = band < 0 ? 0 : band, ke = band < 0 ? h->n_bands : band + 1;
     std::pair<cudaEvent_t, cudaEvent_t> tm;
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
@@ -235,17 +239,19 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
         a.D = h->D;
         a.transpose = transpose;
         const dim3 grid((unsigned)ceil_div(a.nzz, 32), (unsigned)ceil_div(a.nys, 8), a.nxs);
-        if (h->sym && transpose) bp_exact_kernel<true, true><<<grid, dim3(32, 8), 0, st>>>(a);
-        else if (h->sym) bp_exact_kernel<true, false><<<grid, dim3(32, 8), 0, st>>>(a);
-        else if (transpose) bp_exact_kernel<false, true><<<grid, dim3(32, 8), 0, st>>>(a);
-        else bp_exact_kernel<false, false><<<grid, dim3(32, 8), 0, st>>>(a);
-        FDK_CUDA(cudaGetLastError());
-        h->launches++;
-        for (int k = 0; k < h->n_bands; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
+        if (kb == 0) {
+            if (h->sym && transpose) bp_exact_kernel<true, true><<<grid, dim3(32, 8), 0, st>>>(a);
+            else if (h->sym) bp_exact_kernel<true, false><<<grid, dim3(32, 8), 0, st>>>(a);
+            else if (transpose) bp_exact_kernel<false, true><<<grid, dim3(32, 8), 0, st>>>(a);
+            else bp_exact_kernel<false, false><<<grid, dim3(32, 8), 0, st>>>(a);
+            FDK_CUDA(cudaGetLastError());
+            h->launches++;
+        }
+        for (int k = kb; k < ke; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
     } else {
         FDK_CHECK_ARG(layout == FDK_LAYOUT_MIRROR, "fast backprojection reads the MIRROR layout");
         if (h->plan.tma_ok && ((uintptr_t)dev_proj & 15) == 0) {
-            for (int k = 0; k < h->n_bands; k++) {
+            for (int k = kb; k < ke; k++) {
                 if (h->precision == FDK_BP_MIXED)
                     FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
                                                    acc_scale, h->band_tz[k], h->band_tz[k + 1]));
@@ -258,14 +264,16 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
         } else {
             const float ws = weight_scale(host_mats, h->top.x + 0.5f * (h->top.width - 1),
                                           h->top.y + 0.5f * (h->top.height - 1));
-            FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, ws, acc_scale));
-            h->launches++;
-            for (int k = 0; k < h->n_bands; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
+            if (kb == 0) {
+                FDK_TRY(bp_fast_launch(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, n, st, ws, acc_scale));
+                h->launches++;
+            }
+            for (int k = kb; k < ke; k++) FDK_CUDA(cudaEventRecord(h->band_done[k], st));
         }
     }
     FDK_CUDA(cudaEventRecord(tm.second, st));
     h->timers.push_back(tm);
-    h->bp_count += n;
+    if (kb == 0) h->bp_count += n;
     return FDK_OK;
 }
 
@@ -661,9 +669,10 @@ int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale) {
 
 // Backprojection of device-resident views with device-resident matrices, for the
 // reconstructor (recon.cu): no host round trip per batch, so consecutive batches queue on the
-// stream without the host waiting for the GPU.  Internal to the library.
+// stream without the host waiting for the GPU.  band: -1 = the whole volume, else one z band
+// (0 .. fdk_bp_band_count_internal - 1).  Internal to the library.
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
-                                   int32_t n_proj, const float *host_mats, void *stream) {
+                                   int32_t n_proj, const float *host_mats, void *stream, int32_t band) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(h && dev_proj && dev_mats && host_mats, "NULL argument");
     FDK_CHECK_ARG(n_proj > 0 && n_proj <= 128, "n_proj %d outside 1..128", n_proj);
@@ -671,6 +680,9 @@ int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layo
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
     return launch_bp(h, dev_proj, layout, 1, dev_mats, host_mats, n_proj, h->proj_w, h->proj_h,
-                     (cudaStream_t)stream, h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr);
+                     (cudaStream_t)stream, h->precision == FDK_BP_MIXED ? h->ext_scale : nullptr, band);
     FDK_ABI_END
 }
+
+// z bands of a batch (1 where the kernel has none).  Internal to the library (recon.cu).
+int fdk_bp_band_count_internal(const fdk_bp *h) { return h ? h->n_bands : 1; }

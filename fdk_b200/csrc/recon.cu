@@ -8,7 +8,9 @@
 // Views move in chunks of up to 32; the ring holds batch / chunk + 2 chunks, so the copies of
 // the next batch's views land while the current batch's backprojection runs (a slot is free
 // again once its chunk is filtered, and the filters of a batch queue behind the previous
-// batch's backprojection on the compute stream).
+// batch's backprojection on the compute stream).  A full batch is held until the next batch
+// starts, so at the end of a scan two batches wait, and the final flush runs them z band by z
+// band: the volume's first bands are final early and their copy to the host overlaps the rest.
 //
 // The whole volume is one mirror-symmetric slab pair (DivVolume with one rank,
 // cuFDK/mpiFDK.h:116-149): top = z in [0, nz/2), bottom = z in [nz/2, nz).  Host waits are
@@ -40,7 +42,7 @@ struct fdk_recon {
     fdk_toeplitz *tpz = nullptr;     // tensor-core filter (MIXED), else the FFT filter
     int chunk = 32;                  // views per raw slot
     std::vector<float *> d_raw;      // the ring of raw-view slots
-    void *d_filt = nullptr;
+    void *d_filt[2] = {nullptr, nullptr};  // filtered-view batches: the one filling and the held one
     float *d_scale = nullptr;        // accumulator scale of FP16 views (device scalar)
     unsigned int *d_overflow = nullptr;
     float out_scale = 1.0f;
@@ -50,9 +52,14 @@ struct fdk_recon {
     std::vector<cudaEvent_t> raw_ready, raw_free;
     cudaEvent_t done = nullptr;
     int slot = 0;
-    // filtered views waiting in d_filt for a full batch: views pend_first .. pend_first+pending-1
+    // d_filt[cur] is filling: views pend_first .. pend_first+pending-1.  held: d_filt[cur ^ 1]
+    // holds a full batch (views held_first ..) that is backprojected when the next batch starts,
+    // or together with the filling one at a flush (band-interleaved, see flush_all).
+    int cur = 0;
     int pending = 0;
     long long pend_first = 0;
+    bool held = false;
+    long long held_first = 0;
     double filter_ms = 0;
     long long views = 0;
     long long filter_launches = 0;   // kernel launches of the filter since creation or reset
@@ -66,7 +73,8 @@ struct fdk_recon {
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
 long long fdk_bp_launches_internal(const fdk_bp *h);
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
-                                   int32_t n_proj, const float *host_mats, void *stream);
+                                   int32_t n_proj, const float *host_mats, void *stream, int32_t band);
+int fdk_bp_band_count_internal(const fdk_bp *h);
 
 namespace {
 
@@ -94,7 +102,8 @@ int recon_release(fdk_recon *h) {
     }
     if (h->d_cos) cudaFree(h->d_cos);
     if (h->d_mats) cudaFree(h->d_mats);
-    if (h->d_filt) cudaFree(h->d_filt);
+    for (void *p : h->d_filt)
+        if (p) cudaFree(p);
     if (h->d_scale) cudaFree(h->d_scale);
     if (h->d_overflow) cudaFree(h->d_overflow);
     if (h->done) cudaEventDestroy(h->done);
@@ -117,30 +126,62 @@ int collect_filter_timers(fdk_recon *h) {
     return FDK_OK;
 }
 
-// Backproject the filtered views waiting in d_filt (one batch: a launch per z band), on the
-// compute stream.
-int flush_pending(fdk_recon *h) {
-    if (h->pending == 0) return FDK_OK;
-    FDK_TRY(fdk_bp_bp_device_mats_internal(h->bp, h->d_filt, h->layout, h->d_mats + 12 * h->pend_first, h->pending,
-                                           h->mats.data() + 12 * h->pend_first, h->compute));
+// Backproject n filtered views of buffer b starting at view `first`: every z band (band -1) or
+// one, on the compute stream.
+int launch_batch(fdk_recon *h, int b, long long first, int n, int band) {
+    return fdk_bp_bp_device_mats_internal(h->bp, h->d_filt[b], h->layout, h->d_mats + 12 * first, n,
+                                          h->mats.data() + 12 * first, h->compute, band);
+}
+
+// The filling batch is full and more views arrive: backproject the held batch (its launch
+// queues behind the filters already issued, and the next filters write its buffer after it),
+// hold the full one, fill the other buffer.
+int rotate_full(fdk_recon *h) {
+    if (h->held) FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, -1));
+    h->held = true;
+    h->held_first = h->pend_first;
+    h->cur ^= 1;
     h->pending = 0;
     return FDK_OK;
 }
 
-// Filter n raw views (device) into the batch buffer behind the views already waiting there;
-// a full batch is backprojected at once.  Views join a batch only when they continue it
-// (first == pend_first + pending); otherwise the waiting views are backprojected first.
+// Backproject everything waiting.  With two batches waiting (the usual state after the last
+// push of a scan) they run band by band, held then filling: z band 0 has all its views after two
+// band launches instead of after the whole held batch, so a readback (fdk_bp_get_volume) starts
+// early.  Each voxel still receives the held batch's views before the filling batch's.
+int flush_all(fdk_recon *h) {
+    if (h->held && h->pending > 0) {
+        const int nb = fdk_bp_band_count_internal(h->bp);
+        for (int b = 0; b < nb; b++) {
+            FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, b));
+            FDK_TRY(launch_batch(h, h->cur, h->pend_first, h->pending, b));
+        }
+    } else if (h->held) {
+        FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, -1));
+    } else if (h->pending > 0) {
+        FDK_TRY(launch_batch(h, h->cur, h->pend_first, h->pending, -1));
+    }
+    h->held = false;
+    h->pending = 0;
+    return FDK_OK;
+}
+
+// Filter n raw views (device) into the filling batch behind the views already there; a full
+// batch is held until the next one starts (rotate_full).  Views join a batch only when they
+// continue the waiting views (first == the next view expected); otherwise everything waiting
+// is backprojected first.
 int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cudaEvent_t release) {
     const fdk_geometry &g = h->g;
     const long long frame = g.nu * g.nv;
     const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
     const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
-    if (h->pending > 0 && first != h->pend_first + h->pending) FDK_TRY(flush_pending(h));
+    const long long expected = h->pending > 0 ? h->pend_first + h->pending : h->held_first + h->batch;
+    if ((h->pending > 0 || h->held) && first != expected) FDK_TRY(flush_all(h));
     for (int done = 0; done < n;) {
-        if (h->pending == h->batch) FDK_TRY(flush_pending(h));
+        if (h->pending == h->batch) FDK_TRY(rotate_full(h));
         if (h->pending == 0) h->pend_first = first + done;
         const int m = std::min(n - done, h->batch - h->pending);
-        void *dst = static_cast<unsigned char *>(h->d_filt) + (size_t)h->pending * dstride * esz;
+        void *dst = static_cast<unsigned char *>(h->d_filt[h->cur]) + (size_t)h->pending * dstride * esz;
         std::pair<cudaEvent_t, cudaEvent_t> t;  // filter time only (the flush below is the BP's)
         FDK_CUDA(cudaEventCreate(&t.first));
         FDK_CUDA(cudaEventCreate(&t.second));
@@ -159,9 +200,8 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
         done += m;
     }
     if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
-    // the raw views are consumed once filtered: release them before a full batch's launch
+    // the raw views are consumed once filtered
     if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
-    if (h->pending == h->batch) FDK_TRY(flush_pending(h));
     h->views += n;
     return FDK_OK;
 }
@@ -234,7 +274,8 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         ck(cudaEventCreateWithFlags(&h->raw_free[i], cudaEventDisableTiming), "event");
     }
     const size_t esz = h->layout == FDK_LAYOUT_MIRROR ? (h->dtype == FDK_DTYPE_F16 ? 4 : 8) : 4;
-    if (s == FDK_OK) ck(cudaMalloc(&h->d_filt, esz * frame * batch), "filtered views");
+    for (int i = 0; i < 2 && s == FDK_OK; i++)
+        ck(cudaMalloc(&h->d_filt[i], esz * frame * batch), "filtered views");
     if (s == FDK_OK) ck(cudaMalloc(&h->d_overflow, sizeof(unsigned int)), "overflow flag");
     if (s == FDK_OK) ck(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)), "overflow flag");
     if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->compute, cudaStreamNonBlocking), "stream");
@@ -393,7 +434,7 @@ int fdk_recon_flush(fdk_recon *h) {
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    return flush_pending(h);
+    return flush_all(h);
     FDK_ABI_END
 }
 
@@ -402,7 +443,7 @@ int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms) {
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_TRY(flush_pending(h));
+    FDK_TRY(flush_all(h));
     FDK_CUDA(cudaEventRecord(h->done, h->compute));
     const auto t0 = std::chrono::steady_clock::now();
     const int64_t limit = timeout_ms > 0 ? timeout_ms : 600000;
@@ -431,7 +472,7 @@ int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size) {
     {
         DeviceGuard dg(h->device);
         FDK_TRY(dg.status);
-        FDK_TRY(flush_pending(h));
+        FDK_TRY(flush_all(h));
     }
     // band by band, overlapping the last batch's backprojection; then the filter checks
     FDK_TRY(fdk_bp_get_volume(h->bp, host_vol, size));
@@ -474,6 +515,8 @@ int fdk_recon_reset(fdk_recon *h) {
     h->views = 0;
     h->filter_launches = 0;
     h->pending = 0;  // filtered views not yet backprojected are dropped with the volume
+    h->held = false;
+    h->cur = 0;
     return fdk_bp_reset(h->bp);
     FDK_ABI_END
 }

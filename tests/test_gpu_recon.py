@@ -229,8 +229,8 @@ def test_z_bands_and_overlapped_readback(precision, monkeypatch):
             r.push(proj[16:].copy(), 16)
         else:
             r.push(proj.copy(), 0)
-        launches = r.launch_count
         v = r.volume()
+        launches = r.launch_count
         r.close()
         return v, launches
 
