@@ -2,8 +2,9 @@
 """FDK reconstruction benchmark: GUPS at 2048^3 x 4096 views of 2048^2 on B200.
 
 One step = one batch of 32 views through the hot path (the workload streams 32-view batches):
-cosine weight + ramp/Hann filter at once, backprojection into the resident volume once four
-batches (128 views) have been filtered (128 steps = the whole 4096-view reconstruction).
+cosine weight + ramp/Hann filter at once, backprojection into the resident volume in batches of
+256 views (eight steps; a full batch runs when the next one starts, the last two at the final
+flush), 128 steps = the whole 4096-view reconstruction.
 GUPS = nx*ny*nz*views / seconds / 1e9 (the reference's definition, cuFDK/mpiFDK.h:211,
 cudaBP/cudaBP.cpp:68).
 
@@ -164,7 +165,7 @@ def run_reference(args, param, rank: int) -> None:
 
 # --------------------------------------------------------------------------- our arm
 PUSH = 32    # views per step (one filter launch)
-BATCH = 128  # views per backprojection launch (every fourth step)
+BATCH = 256  # views per backprojection batch (every eighth step); --bp-batch changes it
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
@@ -197,15 +198,15 @@ def workload_config(param, args) -> dict:
             "parallelism": f"z-slab pairs x{args.gpus}"}
 
 
-def read_traffic(name: str):
-    """DRAM bytes per backprojection batch (or filter launch) recorded from an ncu capture
-    (profiles/<name>.md line 'dram_bytes_per_batch_full: X' or 'dram_bytes_per_launch_full: X')."""
+def read_traffic(name: str, key: str):
+    """DRAM bytes recorded from an ncu capture: the value of line '<key>: X' in profiles/<name>.md
+    (e.g. dram_bytes_per_256_view_batch_full), or None."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         txt = open(path).read()
     except OSError:
         return None
-    m = re.search(r"dram_bytes_per_(?:launch|batch)_full:\s*([0-9.eE+]+)", txt)
+    m = re.search(rf"{key}:\s*([0-9.eE+]+)", txt)
     return float(m.group(1)) if m else None
 
 
@@ -305,7 +306,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         d = min(64, slab[1])
         vols = {}
         for prec in (args.precision, "fp32"):
-            ra = F.Reconstructor(param, prec, batch=BATCH, device=local, slab=(z0, d))
+            ra = F.Reconstructor(param, prec, batch=64, device=local, slab=(z0, d))  # 64 views
             ra.push_device(views.data_ptr(), 0, min(64, n_dev_views))
             vols[prec] = ra.volume().astype(np.float64)
             ra.close()
@@ -400,7 +401,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             hbm_peak, hbm_src = 6650.0, "fallback"
         bp_batch_ms = bp_ms / n_bp_batches
         bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / n_bp_batches
-        traffic = read_traffic(f"bp_tma_{args.precision}_c2.md")
+        traffic = read_traffic(f"bp_tma_{args.precision}_c2.md", f"dram_bytes_per_{BATCH}_view_batch_full")
         roofline = {
             "kernel": f"bp_tma_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
             if args.precision != "fp32_exact" else "bp_exact_kernel",
@@ -436,7 +437,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
                            "achieved": flt_bytes / (flt_step_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                            "frac": flt_bytes / (flt_step_ms * 1e-3) / 1e9 / hbm_peak,
                            "algorithmic_bytes_per_launch": flt_bytes, "launch_ms": flt_step_ms,
-                           "traffic": read_traffic(f"filter_{args.precision}_c2.md")}
+                           "traffic": read_traffic(f"filter_{args.precision}_c2.md", "dram_bytes_per_launch_full")}
         out = {
             "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -456,6 +457,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
 
 
 def main():
+    global BATCH
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=128)
@@ -463,12 +465,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_exact"])
     ap.add_argument("--config", default="c3")
+    ap.add_argument("--bp-batch", type=int, default=BATCH, help="views per backprojection batch")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    BATCH = args.bp_batch
     from fdk_b200.geometry import config
 
     param = config(args.config)

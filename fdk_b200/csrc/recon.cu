@@ -228,7 +228,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
     FDK_CHECK_ARG(out && g, "NULL argument");
     *out = nullptr;
     FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
-    FDK_CHECK_ARG(batch > 0 && batch <= 128, "batch must be 1..128");
+    FDK_CHECK_ARG(batch > 0 && batch <= 256, "batch must be 1..256");
     FDK_CHECK_ARG(g->nz % 2 == 0, "the slab-pair reconstructor needs an even nz");
     FDK_CHECK_ARG(depth > 0 && top_z >= 0 && top_z + depth <= g->nz / 2, "slab [%lld, %lld) outside the top half",
                   (long long)top_z, (long long)(top_z + depth));
@@ -309,8 +309,10 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         const uint64_t d = (uint64_t)depth, z0 = (uint64_t)top_z;
         fdk_box top{0, 0, z0, (uint64_t)g->nx, (uint64_t)g->ny, d};
         fdk_box bot{0, 0, (uint64_t)g->nz - z0 - d, (uint64_t)g->nx, (uint64_t)g->ny, d};
-        s = fdk_bp_create(&h->bp, (int)g->nv, (int)g->nu, precision == FDK_BP_FP32_EXACT ? 32 : batch, (int)g->nx,
-                          (int)g->ny, (int)g->nz, &top, &bot, precision, device);
+        // the reconstructor feeds the handle device-resident views only (no host-view staging:
+        // a view count of 1 keeps those buffers minimal)
+        s = fdk_bp_create(&h->bp, (int)g->nv, (int)g->nu, 1, (int)g->nx, (int)g->ny, (int)g->nz, &top, &bot,
+                          precision, device);
         if (s == FDK_OK && h->d_scale) s = fdk_bp_set_acc_scale_internal(h->bp, h->d_scale);
     }
     if (s != FDK_OK) {

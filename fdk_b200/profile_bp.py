@@ -17,6 +17,7 @@ prec = sys.argv[1] if len(sys.argv) > 1 else "mixed"
 nb = int(sys.argv[2]) if len(sys.argv) > 2 else 3
 B = int(sys.argv[3]) if len(sys.argv) > 3 else 128
 p = F.config("c2")
+p.nProj = max(p.nProj, B * nb)  # views over the full circle; more when the run asks for more
 views = torch.empty((B * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
 P.project(p, P.phantom_for(p, 2, 20), 0, B * nb, views.data_ptr())
 r = F.Reconstructor(p, prec, batch=B)
