@@ -169,10 +169,12 @@ BATCH = 256  # views per backprojection batch (every eighth step); --bp-batch ch
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
-def count_bp_batches(firsts, n: int) -> int:
+def count_bp_batches(firsts, n: int, batch: int | None = None) -> int:
     """Backprojection batches the reconstructor runs for pushes of n views starting at `firsts`
     (from an empty batch, flushed at the end): one per full batch, per push that does not
-    continue the waiting batch, and the final flush.  A batch is one kernel launch per z band."""
+    continue the waiting batch, and the final flush.  A batch is one kernel launch per z band.
+    batch: views per batch (default: BATCH)."""
+    batch = batch or BATCH
     pending, pf, launches = 0, 0, 0
     for f in firsts:
         if pending and f != pf + pending:
@@ -181,9 +183,9 @@ def count_bp_batches(firsts, n: int) -> int:
         while done < n:
             if pending == 0:
                 pf = f + done
-            m = min(n - done, BATCH - pending)
+            m = min(n - done, batch - pending)
             pending, done = pending + m, done + m
-            if pending == BATCH:
+            if pending == batch:
                 launches, pending = launches + 1, 0
     return launches + (1 if pending else 0)
 

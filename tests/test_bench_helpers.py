@@ -3,17 +3,17 @@ import bench
 
 
 def test_batches_of_in_order_pushes():
-    # 128 steps of 32 views in order: one batch per 4 steps
-    assert bench.count_bp_batches([32 * i for i in range(128)], 32) == 32
+    # 128 steps of 32 views in order, 128-view batches: one batch per 4 steps
+    assert bench.count_bp_batches([32 * i for i in range(128)], 32, 128) == 32
     # a partial last batch is flushed at the end
-    assert bench.count_bp_batches([32 * i for i in range(5)], 32) == 2
+    assert bench.count_bp_batches([32 * i for i in range(5)], 32, 128) == 2
 
 
 def test_batches_break_on_discontinuity():
     # the views restart (the workload wraps around): the waiting batch is backprojected first
-    assert bench.count_bp_batches([0, 32, 0, 32], 32) == 2
+    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128) == 2
     # a push larger than a batch fills several batches
-    assert bench.count_bp_batches([0], 300) == 3
+    assert bench.count_bp_batches([0], 300, 128) == 3
 
 
 class _Done:
