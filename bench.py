@@ -3,7 +3,7 @@
 
 One step = one batch of 32 views through the hot path (the workload streams 32-view batches):
 cosine weight + ramp/Hann filter at once, backprojection into the resident volume in batches of
-256 views (eight steps; a full batch runs when the next one starts, the last two at the final
+512 views (16 steps; a full batch runs when the next one starts, the last two at the final
 flush), 128 steps = the whole 4096-view reconstruction.
 GUPS = nx*ny*nz*views / seconds / 1e9 (the reference's definition, cuFDK/mpiFDK.h:211,
 cudaBP/cudaBP.cpp:68).
@@ -165,7 +165,7 @@ def run_reference(args, param, rank: int) -> None:
 
 # --------------------------------------------------------------------------- our arm
 PUSH = 32    # views per step (one filter launch)
-BATCH = 256  # views per backprojection batch (every eighth step); --bp-batch changes it
+BATCH = 512  # views per backprojection batch (every 16th step); --bp-batch changes it
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 

@@ -675,7 +675,7 @@ int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layo
                                    int32_t n_proj, const float *host_mats, void *stream, int32_t band) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(h && dev_proj && dev_mats && host_mats, "NULL argument");
-    FDK_CHECK_ARG(n_proj > 0 && n_proj <= 256, "n_proj %d outside 1..256", n_proj);
+    FDK_CHECK_ARG(n_proj > 0 && n_proj <= 512, "n_proj %d outside 1..512", n_proj);
     if (h->precision != FDK_BP_FP32_EXACT) FDK_TRY(check_circular(host_mats, n_proj));
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);

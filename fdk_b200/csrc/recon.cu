@@ -228,7 +228,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
     FDK_CHECK_ARG(out && g, "NULL argument");
     *out = nullptr;
     FDK_CHECK_ARG(precision >= FDK_BP_FP32_EXACT && precision <= FDK_BP_MIXED, "bad precision");
-    FDK_CHECK_ARG(batch > 0 && batch <= 256, "batch must be 1..256");
+    FDK_CHECK_ARG(batch > 0 && batch <= 512, "batch must be 1..512");
     FDK_CHECK_ARG(g->nz % 2 == 0, "the slab-pair reconstructor needs an even nz");
     FDK_CHECK_ARG(depth > 0 && top_z >= 0 && top_z + depth <= g->nz / 2, "slab [%lld, %lld) outside the top half",
                   (long long)top_z, (long long)(top_z + depth));

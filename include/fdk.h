@@ -246,7 +246,7 @@ int fdk_rtk_sync(void *stream);
 typedef struct fdk_recon fdk_recon;
 /* A reconstructor for geometry g: cosine weight + ramp filter + backprojection of the whole
  * volume (mirror slab pair, as DivVolume with one rank, cuFDK/mpiFDK.h:116-149).
- * batch: views per backprojection batch (<= 256; <= 32 for FDK_BP_FP32_EXACT), independent of
+ * batch: views per backprojection batch (<= 512; <= 32 for FDK_BP_FP32_EXACT), independent of
  * how many views each push carries.  Two batches of filtered views stay on the device.
  * precision: FDK_BP_*. */
 int fdk_recon_create(fdk_recon **out, const fdk_geometry *g, int32_t precision, int32_t batch,

@@ -287,3 +287,26 @@ def test_rtk_staged_kernel_matches_l1_and_oracle(case, monkeypatch):
     assert torch.equal(staged, l1)
     want = O.rtk_bp(proj, mats, vin.cpu().numpy())
     assert rel_l2(staged.cpu().numpy(), want) <= 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp32", "mixed"])
+def test_largest_batches_match_small_ones(precision):
+    """Batches of the largest size (512 views; two are held on the device) give the volume of
+    16-view batches up to FP32 summation order, over a scan longer than one batch."""
+    import torch
+
+    n, views = 32, 600
+    p = small_param(n, 48, 40, views)
+    dev = torch.empty((views, 40, 48), dtype=torch.float32, device="cuda")
+    project(p, phantom_for(p, 9, 12), 0, views, dev.data_ptr())
+    torch.cuda.synchronize()
+    proj = dev.cpu().numpy()
+    vols = []
+    for batch in (512, 16):
+        r = F.Reconstructor(p, precision, batch=batch)
+        for c in range(0, views, 32):
+            r.push(proj[c:c + 32].copy(), c)
+        vols.append(r.volume())
+        assert r.stats()["views"] == views
+        r.close()
+    assert rel_l2(vols[0], vols[1]) <= 1e-5
