@@ -52,7 +52,8 @@ class Reconstructor:
         return "tensor" if k.value == 1 else "fft"
 
     def flush(self) -> None:
-        """Backproject the filtered views waiting for a full batch now (asynchronous)."""
+        """Backproject every filtered view still waiting (a held full batch and the filling one)
+        now (asynchronous)."""
         check(lib().fdk_recon_flush(self._h))
 
     def push_folder(self, folder: str, first: int, n: int, step: int = 1, start: int = 0, threads: int = 0) -> None:

@@ -271,9 +271,11 @@ int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, i
  * batch k.  Every file's size is checked before any is read (FDK_ERR_IO names the first bad one). */
 int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64_t n, int32_t step,
                           int32_t start, int32_t threads);
-/* Pushed views are filtered at once and backprojected a full batch at a time (views that do not
- * continue the waiting batch close it first).  fdk_recon_flush launches the backprojection of a
- * partial batch now (asynchronous); fdk_recon_sync and fdk_recon_get_volume flush implicitly. */
+/* Pushed views are filtered at once and backprojected a full batch at a time; a full batch runs
+ * when the next batch starts (views that do not continue the waiting ones close them first).
+ * fdk_recon_flush launches the backprojection of everything waiting now (asynchronous; two
+ * waiting batches run z band by z band); fdk_recon_sync and fdk_recon_get_volume flush
+ * implicitly. */
 int fdk_recon_flush(fdk_recon *h);
 /* The row filter this reconstructor runs: 0 the FFT filter (fdk_filter_*), 1 the split-FP16
  * tensor-core GEMM (fdk_toeplitz_*, MIXED precision when nu % 256 == 0 and nv % 128 == 0 on an
