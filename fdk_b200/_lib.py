@@ -39,11 +39,11 @@ EXPORTED = [
     "fdk_filter_create", "fdk_filter_filtering", "fdk_filter_run_device", "fdk_filter_destroy",
     "fdk_correct_image_real32", "fdk_filter_row_real32", "fdk_filter_row_real32_noalloc",
     "fdk_bp_create", "fdk_bp_bp", "fdk_bp_bp_device", "fdk_bp_get_volume", "fdk_bp_volume_device",
-    "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
+    "fdk_bp_sample", "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
     "fdk_rtk_reconstruct_conebeam", "fdk_rtk_backproject_device", "fdk_rtk_sync",
     "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device",
     "fdk_recon_push_folder", "fdk_recon_flush", "fdk_recon_filter_kind", "fdk_recon_sync",
-    "fdk_recon_get_volume", "fdk_recon_stats", "fdk_recon_launch_count", "fdk_recon_reset", "fdk_recon_destroy",
+    "fdk_recon_get_volume", "fdk_recon_sample", "fdk_recon_stats", "fdk_recon_launch_count", "fdk_recon_reset", "fdk_recon_destroy",
     "fdk_phantom_project", "fdk_forward_project", "fdk_probe_smem", "fdk_probe_fma",
     "fdk_nn_param_count", "fdk_nn_forward", "fdk_nn_backward", "fdk_adam_step", "fdk_transmission_noise",
     "fdk_voxelize", "fdk_rows_to_mirror", "fdk_volume_mse", "fdk_bp_adjoint",
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
         "fdk_bp_bp_device": ([vp, vp, i32, vp, i32, vp], C.c_int),
         "fdk_bp_get_volume": ([vp, vp, i64], C.c_int),
         "fdk_bp_volume_device": ([vp, C.POINTER(vp), C.POINTER(i64)], C.c_int),
+        "fdk_bp_sample": ([vp, vp, i64, vp], C.c_int),
         "fdk_bp_stats": ([vp, C.POINTER(i64), f64p], C.c_int),
         "fdk_bp_reset": ([vp], C.c_int),
         "fdk_bp_destroy": ([vp], C.c_int),
@@ -142,6 +143,7 @@ def lib() -> C.CDLL:
         "fdk_recon_filter_kind": ([vp, C.POINTER(i32)], C.c_int),
         "fdk_recon_sync": ([vp, i64], C.c_int),
         "fdk_recon_get_volume": ([vp, vp, i64], C.c_int),
+        "fdk_recon_sample": ([vp, vp, i64, vp], C.c_int),
         "fdk_recon_stats": ([vp, f64p, f64p, C.POINTER(i64)], C.c_int),
         "fdk_recon_launch_count": ([vp, C.POINTER(i64)], C.c_int),
         "fdk_recon_reset": ([vp], C.c_int),

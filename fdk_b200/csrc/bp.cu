@@ -131,6 +131,27 @@ __global__ void transpose_views_kernel(const float *__restrict__ src, float *__r
     }
 }
 
+// Gather listed voxels (x, y, z of the whole volume) from the slab-pair volume [x][y][zs];
+// voxels outside the handle's boxes read NaN.  MIXED folds its compensation term.
+__global__ void sample_voxels_kernel(const float *__restrict__ vol, const float *__restrict__ comp,
+                                     const int *__restrict__ xyz, long long n, float *__restrict__ out, int x0,
+                                     int y0, int nxs, int nys, long long tz0, long long td, long long bz0,
+                                     long long bd, long long D) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = xyz[3 * i] - x0, y = xyz[3 * i + 1] - y0;
+        const long long z = xyz[3 * i + 2];
+        long long zs = -1;
+        if (z >= tz0 && z < tz0 + td) zs = z - tz0;
+        else if (bd > 0 && z >= bz0 && z < bz0 + bd) zs = td + (z - bz0);
+        float v = __int_as_float(0x7fc00000);
+        if (zs >= 0 && x >= 0 && x < nxs && y >= 0 && y < nys) {
+            const long long o = ((long long)x * nys + y) * D + zs;
+            v = comp ? vol[o] - comp[o] : vol[o];
+        }
+        out[i] = v;
+    }
+}
+
 }  // namespace fdk
 
 using namespace fdk;
@@ -177,13 +198,15 @@ struct fdk_bp {
     float *d_rb = nullptr;                    // readback staging, 2 x rb_planes z planes
     long long rb_planes = 0;
     long long launches = 0;                   // kernel launches since creation or reset
+    cudaEvent_t sync_ev[3] = {};              // scratch events of the bounded host waits
+    unsigned int *h_err = nullptr;            // pinned host copy of the device error word
 };
 
 namespace bpi {
 
 int collect_timers(fdk_bp *h) {
     for (auto &t : h->timers) {
-        FDK_CUDA(cudaEventSynchronize(t.second));
+        FDK_TRY(wait_event(t.second, "backprojection"));
         float ms = 0;
         FDK_CUDA(cudaEventElapsedTime(&ms, t.first, t.second));
         h->kernel_ms += ms;
@@ -277,13 +300,16 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
     return FDK_OK;
 }
 
-// The TMA kernel's bounded waits report through a device error word; read it after a sync.
+// The TMA kernel's bounded waits report through a device error word; read it (on the handle's
+// stream, a bounded wait) once the kernels that may set it have finished.
 int check_device_error(fdk_bp *h) {
     if (!h->plan.d_err) return FDK_OK;
-    unsigned int e = 0;
-    FDK_CUDA(cudaMemcpy(&e, h->plan.d_err, sizeof(e), cudaMemcpyDeviceToHost));
+    FDK_CUDA(cudaMemcpyAsync(h->h_err, h->plan.d_err, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    FDK_TRY(wait_stream(h->stream, h->sync_ev[2], "error word"));
+    const unsigned int e = *h->h_err;
     if (e) {
-        cudaMemset(h->plan.d_err, 0, sizeof(e));
+        FDK_CUDA(cudaMemsetAsync(h->plan.d_err, 0, sizeof(e), h->stream));
+        FDK_TRY(wait_stream(h->stream, h->sync_ev[2], "error word"));
         return fail(FDK_ERR_DEVICE_CHECK, "backprojection pipeline wait timed out on the device (error word %u)", e);
     }
     return FDK_OK;
@@ -332,8 +358,8 @@ int read_volume(fdk_bp *h, float *host) {
             FDK_CUDA(cudaMemcpyAsync(host + plane * z, buf, sizeof(float) * plane * n, cudaMemcpyDeviceToHost, st));
         }
     }
-    FDK_CUDA(cudaStreamSynchronize(h->rb[0]));
-    FDK_CUDA(cudaStreamSynchronize(h->rb[1]));
+    FDK_TRY(wait_stream(h->rb[0], h->sync_ev[0], "volume readback"));
+    FDK_TRY(wait_stream(h->rb[1], h->sync_ev[1], "volume readback"));
     return FDK_OK;
 }
 
@@ -398,7 +424,9 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
     };
     ck(cudaMalloc(&h->d_vol, sizeof(float) * nvox), "volume");
-    if (s == FDK_OK) ck(cudaMemset(h->d_vol, 0, sizeof(float) * nvox), "volume zero");
+    for (int i = 0; i < 3 && s == FDK_OK; i++)
+        ck(cudaEventCreateWithFlags(&h->sync_ev[i], cudaEventDisableTiming), "event");
+    if (s == FDK_OK) ck(cudaHostAlloc((void **)&h->h_err, sizeof(unsigned int), 0), "error word");
     for (int i = 0; i < 2 && s == FDK_OK; i++) {
         ck(cudaMalloc(&h->d_stage[i], sizeof(float) * frame * proj_count), "view staging");
         ck(cudaEventCreateWithFlags(&h->copied[i], cudaEventDisableTiming), "event");
@@ -407,17 +435,18 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
     if (s == FDK_OK) ck(cudaMalloc(&h->d_mats, sizeof(float) * 2 * 128 * 12), "matrices");
     if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
     if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking), "copy stream");
+    if (s == FDK_OK) ck(cudaMemsetAsync(h->d_vol, 0, sizeof(float) * nvox, h->stream), "volume zero");
     if (s == FDK_OK && precision != FDK_BP_FP32_EXACT) {
         const size_t esz = precision == FDK_BP_MIXED ? sizeof(__half2) : sizeof(float2);
         ck(cudaMalloc(&h->d_mirror, esz * frame * proj_count), "mirror staging");
         if (s == FDK_OK && precision == FDK_BP_MIXED) {
             ck(cudaMalloc(&h->d_absmax, sizeof(unsigned int)), "absmax");
             ck(cudaMalloc(&h->d_comp, sizeof(float) * nvox), "compensation");
-            if (s == FDK_OK) ck(cudaMemset(h->d_comp, 0, sizeof(float) * nvox), "compensation zero");
+            if (s == FDK_OK) ck(cudaMemsetAsync(h->d_comp, 0, sizeof(float) * nvox, h->stream), "compensation zero");
         }
         if (s == FDK_OK)
             s = bp_fast_plan(h->plan, precision, proj_width, proj_height, (int)t.x, (int)t.y, (int)t.z,
-                             (int)t.width, (int)t.height, (int)t.depth, h->D, device);
+                             (int)t.width, (int)t.height, (int)t.depth, h->D, device, h->stream);
         if (s == FDK_OK) {
             // The TMA kernel needs 16-byte row strides; FDK_BP_KERNEL=staged selects the
             // synchronous-staging kernel instead (kept for comparison and as the fallback).
@@ -427,7 +456,7 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
                 s = precision == FDK_BP_MIXED ? tma_prepare<__half2>(h->plan.tma_ctas, device)
                                               : tma_prepare<float2>(h->plan.tma_ctas, device);
                 if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
-                if (s == FDK_OK) ck(cudaMemset(h->plan.d_err, 0, sizeof(unsigned int)), "error word");
+                if (s == FDK_OK) ck(cudaMemsetAsync(h->plan.d_err, 0, sizeof(unsigned int), h->stream), "error word");
             }
         }
     }
@@ -463,9 +492,9 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         h->rb_planes = std::max(1ll, std::min(h->D, want));
         ck(cudaMalloc(&h->d_rb, sizeof(float) * 2 * plane * h->rb_planes), "readback staging");
     }
-    // the zeroed volume is in place before any readback (those streams do not order after the
-    // default stream)
-    if (s == FDK_OK) ck(cudaDeviceSynchronize(), "create");
+    // the zeroed volume, the error word and the scale are in place before any readback or launch
+    // on another stream: a bounded wait for the handle's stream, not for the device
+    if (s == FDK_OK) s = wait_stream(h->stream, h->sync_ev[0], "fdk_bp_create");
     if (s != FDK_OK) {
         fdk_bp_destroy(h);
         return s;
@@ -501,7 +530,7 @@ int fdk_bp_bp(fdk_bp *h, int32_t transpose, const float *host_proj, int32_t widt
     FDK_CUDA(cudaMemcpyAsync(d_mats, proj_mat, sizeof(float) * 12 * n_proj, cudaMemcpyHostToDevice, h->copy_stream));
     FDK_CUDA(cudaEventRecord(h->copied[k], h->copy_stream));
     // The caller may reuse host_proj on return: wait for the copy (not for the kernel).
-    FDK_CUDA(cudaEventSynchronize(h->copied[k]));
+    FDK_TRY(wait_event(h->copied[k], "view copy"));
     FDK_CUDA(cudaStreamWaitEvent(h->stream, h->copied[k], 0));
     if (h->precision == FDK_BP_FP32_EXACT) {
         FDK_TRY(launch_bp(h, h->d_stage[k], transpose ? FDK_LAYOUT_TRANSPOSED : FDK_LAYOUT_ROWS, transpose, d_mats,
@@ -572,14 +601,49 @@ int fdk_bp_volume_device(fdk_bp *h, float **dev_vol, int64_t *count) {
     FDK_CHECK_ARG(h && dev_vol && count, "NULL argument");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_CUDA(cudaDeviceSynchronize());
+    FDK_TRY(collect_timers(h));  // every launch of the handle has finished (bounded waits)
     FDK_TRY(check_device_error(h));
     const long long nvox = (long long)h->top.width * h->top.height * h->D;
     if (h->d_comp) FDK_TRY(bp_fast_fold_compensation(h->d_vol, h->d_comp, nvox, h->stream));
-    FDK_CUDA(cudaStreamSynchronize(h->stream));
+    FDK_TRY(wait_stream(h->stream, h->sync_ev[0], "fdk_bp_volume_device"));
     *dev_vol = h->d_vol;
     *count = nvox;
     return FDK_OK;
+    FDK_ABI_END
+}
+
+int fdk_bp_sample(fdk_bp *h, const int32_t *host_xyz, int64_t n, float *host_out) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_xyz && host_out && n >= 0, "NULL argument or negative count");
+    if (n == 0) return FDK_OK;
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(collect_timers(h));  // every launch of the handle has finished (bounded waits)
+    FDK_TRY(check_device_error(h));
+    int *d_xyz = nullptr;
+    float *d_out = nullptr;
+    int s = cuda_status(cudaMalloc(&d_xyz, sizeof(int) * 3 * n), "sample indices", __FILE__, __LINE__);
+    if (s == FDK_OK) s = cuda_status(cudaMalloc(&d_out, sizeof(float) * n), "sample values", __FILE__, __LINE__);
+    if (s == FDK_OK)
+        s = cuda_status(cudaMemcpyAsync(d_xyz, host_xyz, sizeof(int) * 3 * n, cudaMemcpyHostToDevice, h->stream),
+                        "sample indices", __FILE__, __LINE__);
+    if (s == FDK_OK) {
+        const int grid = (int)std::min<long long>(ceil_div(n, 256), 148 * 8);
+        sample_voxels_kernel<<<grid, 256, 0, h->stream>>>(
+            h->d_vol, h->d_comp, d_xyz, n, d_out, (int)h->top.x, (int)h->top.y, (int)h->top.width,
+            (int)h->top.height, (long long)h->top.z, (long long)h->top.depth, (long long)h->bottom.z,
+            h->sym ? (long long)h->bottom.depth : 0ll, h->D);
+        s = cuda_status(cudaGetLastError(), "sample kernel", __FILE__, __LINE__);
+    }
+    if (s == FDK_OK)
+        s = cuda_status(cudaMemcpyAsync(host_out, d_out, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream),
+                        "sample values", __FILE__, __LINE__);
+    if (s == FDK_OK) s = wait_stream(h->stream, h->sync_ev[0], "fdk_bp_sample");
+    cudaStreamSynchronize(h->stream);  // error paths: the buffers are freed below
+    cudaFree(d_xyz);
+    cudaFree(d_out);
+    return s;
     FDK_ABI_END
 }
 
@@ -601,12 +665,12 @@ int fdk_bp_reset(fdk_bp *h) {
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_CUDA(cudaDeviceSynchronize());
+    FDK_TRY(collect_timers(h));  // every launch of the handle has finished (bounded waits)
     const size_t nvox = (size_t)h->top.width * h->top.height * h->D;
-    FDK_CUDA(cudaMemset(h->d_vol, 0, sizeof(float) * nvox));
-    if (h->d_comp) FDK_CUDA(cudaMemset(h->d_comp, 0, sizeof(float) * nvox));
-    FDK_CUDA(cudaDeviceSynchronize());  // the readback streams do not order after the default stream
-    FDK_TRY(collect_timers(h));
+    FDK_CUDA(cudaMemsetAsync(h->d_vol, 0, sizeof(float) * nvox, h->stream));
+    if (h->d_comp) FDK_CUDA(cudaMemsetAsync(h->d_comp, 0, sizeof(float) * nvox, h->stream));
+    // zeroed before the next launch or readback on another stream
+    FDK_TRY(wait_stream(h->stream, h->sync_ev[0], "fdk_bp_reset"));
     h->bp_count = 0;
     h->kernel_ms = 0;
     h->launches = 0;
@@ -647,6 +711,9 @@ int fdk_bp_destroy(fdk_bp *h) {
                 cudaStreamDestroy(h->rb[i]);
             }
         if (h->d_rb) cudaFree(h->d_rb);
+        for (int i = 0; i < 3; i++)
+            if (h->sync_ev[i]) cudaEventDestroy(h->sync_ev[i]);
+        if (h->h_err) cudaFreeHost(h->h_err);
         if (h->stream) cudaStreamDestroy(h->stream);
         if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
     }

@@ -305,7 +305,7 @@ inline int bp_fast_fold_compensation(float *vol, float *comp, long long n, cudaS
 }
 
 inline int bp_fast_plan(BpFastPlan &p, int precision, int proj_w, int proj_h, int x0, int y0, int z0, int nxs,
-                        int nys, int depth_top, long long D, int device) {
+                        int nys, int depth_top, long long D, int device, cudaStream_t st) {
     p.precision = precision;
     p.nv = proj_w;  // transposed frame: width = detector rows
     p.nu = proj_h;
@@ -319,7 +319,7 @@ inline int bp_fast_plan(BpFastPlan &p, int precision, int proj_w, int proj_h, in
     p.device = device;
     FDK_CUDA(cudaMalloc(&p.d_scale, sizeof(float)));
     const float one = 1.0f;
-    FDK_CUDA(cudaMemcpy(p.d_scale, &one, sizeof(float), cudaMemcpyHostToDevice));
+    FDK_CUDA(cudaMemcpyAsync(p.d_scale, &one, sizeof(float), cudaMemcpyHostToDevice, st));  // pageable: staged now
     const size_t smem = (size_t)kFastNch * kFastBoxH * kFastBoxW * (precision == FDK_BP_MIXED ? 4 : 8);
     if (precision == FDK_BP_MIXED)
         FDK_CUDA(cudaFuncSetAttribute(bp_fast_kernel<__half2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

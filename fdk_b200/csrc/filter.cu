@@ -399,10 +399,12 @@ int FilterTables::create(const double *H, int W_) {
     FDK_CUDA(cudaMalloc(&tw, sizeof(float2) * (W / 2)));
     FDK_CUDA(cudaMalloc(&hb, sizeof(float) * W));
     FDK_CUDA(cudaMalloc(&twp, sizeof(float2) * pt.size()));
-    FDK_CUDA(cudaMemcpy(tw, t.data(), sizeof(float2) * (W / 2), cudaMemcpyHostToDevice));
-    FDK_CUDA(cudaMemcpy(hb, h.data(), sizeof(float) * W, cudaMemcpyHostToDevice));
-    FDK_CUDA(cudaMemcpy(twp, pt.data(), sizeof(float2) * pt.size(), cudaMemcpyHostToDevice));
-    return FDK_OK;
+    SetupStream ss;
+    FDK_TRY(ss.open());
+    FDK_CUDA(cudaMemcpyAsync(tw, t.data(), sizeof(float2) * (W / 2), cudaMemcpyHostToDevice, ss.st));
+    FDK_CUDA(cudaMemcpyAsync(hb, h.data(), sizeof(float) * W, cudaMemcpyHostToDevice, ss.st));
+    FDK_CUDA(cudaMemcpyAsync(twp, pt.data(), sizeof(float2) * pt.size(), cudaMemcpyHostToDevice, ss.st));
+    return ss.finish("filter tables");
 }
 
 void FilterTables::release() {
@@ -549,9 +551,14 @@ int fdk_filter_create(fdk_filter **out, const float *cos_table, const float *H, 
     std::vector<double> Hd(H, H + W);
     int s = h->tables.create(Hd.data(), (int)W);
     if (s == FDK_OK && cos_table) {
-        cudaError_t e = cudaMalloc(&h->d_cos, sizeof(float) * nu * nv);
-        if (e == cudaSuccess) e = cudaMemcpy(h->d_cos, cos_table, sizeof(float) * nu * nv, cudaMemcpyHostToDevice);
+        SetupStream ss;
+        s = ss.open();
+        cudaError_t e = cudaSuccess;
+        if (s == FDK_OK) e = cudaMalloc(&h->d_cos, sizeof(float) * nu * nv);
+        if (s == FDK_OK && e == cudaSuccess)
+            e = cudaMemcpyAsync(h->d_cos, cos_table, sizeof(float) * nu * nv, cudaMemcpyHostToDevice, ss.st);
         if (e != cudaSuccess) s = cuda_status(e, "filter cos table", __FILE__, __LINE__);
+        if (s == FDK_OK) s = ss.finish("filter cos table");
     }
     if (s == FDK_OK) {
         cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
@@ -638,10 +645,10 @@ int fdk_correct_image_real32(const fdk_dataref *src, const fdk_dataref *table, f
     FDK_CHECK_ARG(src->width > 0 && src->height > 0 && src->depth > 0 && src->pitch >= src->width, "bad shape");
     FDK_CHECK_ARG(src->height <= 65535 && src->depth <= 65535, "shape too large");
     const dim3 grid((unsigned)ceil_div(src->width, 128), src->height, src->depth);
-    correct_kernel<<<grid, 128>>>(src->data, dst->data, src->pitch, src->width, src->height, src->depth,
-                                  table->data, table->pitch);
+    correct_kernel<<<grid, 128, 0, cudaStreamLegacy>>>(src->data, dst->data, src->pitch, src->width, src->height,
+                                                       src->depth, table->data, table->pitch);
     FDK_CUDA(cudaGetLastError());
-    FDK_CUDA(cudaDeviceSynchronize());
+    FDK_CUDA(cudaStreamSynchronize(cudaStreamLegacy));  // synchronous, as the reference
     return FDK_OK;
     FDK_ABI_END
 }
@@ -663,9 +670,9 @@ int fdk_filter_row_real32(const fdk_dataref *src, fdk_dataref *dst, const fdk_da
     if (s == FDK_OK)
         s = filter_views(src->data, src->pitch, (long long)src->pitch * src->height, dst->data, dst->pitch,
                          (long long)dst->pitch * dst->height, nullptr, 0, t, src->width, src->height, 3,
-                         src->depth, FDK_LAYOUT_ROWS, FDK_DTYPE_F32, 0);
+                         src->depth, FDK_LAYOUT_ROWS, FDK_DTYPE_F32, cudaStreamLegacy);
     if (s == FDK_OK) {
-        cudaError_t e = cudaDeviceSynchronize();
+        cudaError_t e = cudaStreamSynchronize(cudaStreamLegacy);  // synchronous, as the reference
         if (e != cudaSuccess) s = cuda_status(e, "FilterRow sync", __FILE__, __LINE__);
     }
     t.release();

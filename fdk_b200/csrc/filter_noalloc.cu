@@ -16,9 +16,13 @@
 //     reads before its filter kernel runs (nothing needs to start at zero), and the call returns
 //     only after its kernels finish; calls that overlap on the GPU (several host threads calling
 //     at once on one device) race on the tables and must be serialised by the caller.
-//   * The first call on a device looks up the array's device address (cudaGetSymbolAddress, with
-//     that device current) and caches it; that first call should come before any stream capture
-//     begins on the calling thread.
+//   * Set-up: every call looks up the array's device address on the caller's current device
+//     (cudaGetSymbolAddress, return code checked) instead of keeping one from an earlier call,
+//     so a pointer never outlives the context it was taken in (cudaDeviceReset, another
+//     context on the same device).  The first call on a device also loads the library's device
+//     code there; make that first call before any stream capture begins.
+//   * Kernels run on the legacy default stream and the call waits for that stream only (the
+//     reference's FilterRow_Real32 is synchronous too), not for the whole device.
 #include <cuda_runtime.h>
 
 #include "common.h"
@@ -27,7 +31,6 @@
 namespace fdk {
 
 constexpr int kNoAllocMaxW = 4096;
-constexpr int kMaxDevices = 64;
 
 // W/2 float2 twiddles followed by W floats of the bit-reversed response: 4096 * 8 bytes.
 static __device__ __align__(256) float2 g_filter_scratch[kNoAllocMaxW];
@@ -45,17 +48,12 @@ __global__ void build_filter_tables_kernel(const float *__restrict__ H, int W, i
     }
 }
 
+// The array's device address on the current device.  A host-side lookup, repeated per call.
 static int scratch_address(float2 **out) {
-    static float2 *addr[kMaxDevices] = {};
-    int dev = 0;
-    FDK_CUDA(cudaGetDevice(&dev));
-    FDK_CHECK_ARG(dev >= 0 && dev < kMaxDevices, "device index %d out of range", dev);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        FDK_CUDA(cudaGetSymbolAddress(&p, g_filter_scratch));
-        addr[dev] = static_cast<float2 *>(p);
-    }
-    *out = addr[dev];
+    void *p = nullptr;
+    FDK_CUDA(cudaGetSymbolAddress(&p, g_filter_scratch));
+    FDK_CHECK_ARG(p != nullptr, "no device address for the filter tables");
+    *out = static_cast<float2 *>(p);
     return FDK_OK;
 }
 
@@ -86,12 +84,12 @@ extern "C" int fdk_filter_row_real32_noalloc(const fdk_dataref *src, fdk_dataref
     while ((1 << t.log2W) < W) t.log2W++;
     t.tw = scratch;
     t.hb = reinterpret_cast<float *>(scratch + W / 2);
-    build_filter_tables_kernel<<<(W + 255) / 256, 256>>>(filter->data, W, t.log2W, t.tw, t.hb);
+    build_filter_tables_kernel<<<(W + 255) / 256, 256, 0, cudaStreamLegacy>>>(filter->data, W, t.log2W, t.tw, t.hb);
     FDK_CUDA(cudaGetLastError());
     FDK_TRY(filter_views(src->data, src->pitch, (long long)src->pitch * src->height, dst->data, dst->pitch,
                          (long long)dst->pitch * dst->height, nullptr, 0, t, src->width, src->height, 3, src->depth,
-                         FDK_LAYOUT_ROWS, FDK_DTYPE_F32, 0));
-    FDK_CUDA(cudaDeviceSynchronize());
+                         FDK_LAYOUT_ROWS, FDK_DTYPE_F32, cudaStreamLegacy));
+    FDK_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     return FDK_OK;
     FDK_ABI_END
 }

@@ -15,6 +15,7 @@ struct FilterTables {
     float2 *tw = nullptr;
     float2 *twp = nullptr;  // per FFT pass and group, the group's twiddles (optional)
     float *hb = nullptr;
+    // the copies go through a private set-up stream that the call waits for (bounded)
     int create(const double *H, int W_);
     void release();
 };

@@ -67,6 +67,8 @@ struct fdk_recon {
     // pinned staging of fdk_recon_push_folder (allocated on first use): two chunks
     float *h_stage[2] = {nullptr, nullptr};
     cudaEvent_t stage_free[2] = {nullptr, nullptr};
+    cudaEvent_t sync_ev[2] = {nullptr, nullptr};  // scratch events of the bounded host waits
+    unsigned int *h_word = nullptr;               // pinned host copy of the overflow flag
 };
 
 // internal hooks (bp.cu)
@@ -107,6 +109,9 @@ int recon_release(fdk_recon *h) {
     if (h->d_scale) cudaFree(h->d_scale);
     if (h->d_overflow) cudaFree(h->d_overflow);
     if (h->done) cudaEventDestroy(h->done);
+    for (cudaEvent_t e : h->sync_ev)
+        if (e) cudaEventDestroy(e);
+    if (h->h_word) cudaFreeHost(h->h_word);
     if (h->compute) cudaStreamDestroy(h->compute);
     if (h->copy) cudaStreamDestroy(h->copy);
     delete h;
@@ -115,7 +120,7 @@ int recon_release(fdk_recon *h) {
 
 int collect_filter_timers(fdk_recon *h) {
     for (auto &t : h->ftimers) {
-        FDK_CUDA(cudaEventSynchronize(t.second));
+        FDK_TRY(wait_event(t.second, "filter"));
         float ms = 0;
         FDK_CUDA(cudaEventElapsedTime(&ms, t.first, t.second));
         h->filter_ms += ms;
@@ -249,20 +254,30 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
     auto ck = [&](cudaError_t e, const char *what) {
         if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
     };
+    // the set-up copies below queue on the compute stream; the call waits for it at its end
+    ck(cudaStreamCreateWithFlags(&h->compute, cudaStreamNonBlocking), "stream");
+    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "stream");
+    for (int i = 0; i < 2 && s == FDK_OK; i++)
+        ck(cudaEventCreateWithFlags(&h->sync_ev[i], cudaEventDisableTiming), "event");
+    if (s == FDK_OK) ck(cudaHostAlloc((void **)&h->h_word, sizeof(unsigned int), 0), "pinned word");
     // geometry tables (FP64 -> FP32)
     std::vector<double> H(W);
     std::vector<float> cos(g->nu * g->nv);
     h->mats.resize(12 * g->n_proj);
-    s = fdk_filter_design(g->filter_type, g->nu, 1, H.data(), W);
+    if (s == FDK_OK) s = fdk_filter_design(g->filter_type, g->nu, 1, H.data(), W);
     if (s == FDK_OK) s = fdk_cos_table(g, cos.data());
     if (s == FDK_OK) s = fdk_projection_matrices(g, nullptr, h->mats.data());
     if (s == FDK_OK) s = h->tables.create(H.data(), (int)W);
     const long long frame = g->nu * g->nv;
     if (s == FDK_OK) ck(cudaMalloc(&h->d_cos, sizeof(float) * frame), "cos table");
-    if (s == FDK_OK) ck(cudaMemcpy(h->d_cos, cos.data(), sizeof(float) * frame, cudaMemcpyHostToDevice), "cos copy");
+    if (s == FDK_OK)
+        ck(cudaMemcpyAsync(h->d_cos, cos.data(), sizeof(float) * frame, cudaMemcpyHostToDevice, h->compute),
+           "cos copy");
     if (s == FDK_OK) ck(cudaMalloc(&h->d_mats, sizeof(float) * h->mats.size()), "matrices");
     if (s == FDK_OK)
-        ck(cudaMemcpy(h->d_mats, h->mats.data(), sizeof(float) * h->mats.size(), cudaMemcpyHostToDevice), "matrices");
+        ck(cudaMemcpyAsync(h->d_mats, h->mats.data(), sizeof(float) * h->mats.size(), cudaMemcpyHostToDevice,
+                           h->compute),
+           "matrices");
     h->chunk = std::min(batch, 32);
     const int n_slots = (batch + h->chunk - 1) / h->chunk + 2;
     h->d_raw.assign(n_slots, nullptr);
@@ -277,9 +292,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
     for (int i = 0; i < 2 && s == FDK_OK; i++)
         ck(cudaMalloc(&h->d_filt[i], esz * frame * batch), "filtered views");
     if (s == FDK_OK) ck(cudaMalloc(&h->d_overflow, sizeof(unsigned int)), "overflow flag");
-    if (s == FDK_OK) ck(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)), "overflow flag");
-    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->compute, cudaStreamNonBlocking), "stream");
-    if (s == FDK_OK) ck(cudaStreamCreateWithFlags(&h->copy, cudaStreamNonBlocking), "stream");
+    if (s == FDK_OK) ck(cudaMemsetAsync(h->d_overflow, 0, sizeof(unsigned int), h->compute), "overflow flag");
     if (s == FDK_OK) ck(cudaEventCreateWithFlags(&h->done, cudaEventDisableTiming), "event");
     if (s == FDK_OK && h->dtype == FDK_DTYPE_F16) {
         // FP16 views hold the filtered values divided by the cosine table's SOD^2 * AAF factor
@@ -289,7 +302,8 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         const float k = (float)(g->sod * g->sod * aaf);
         h->out_scale = 1.0f / k;
         if (s == FDK_OK) ck(cudaMalloc(&h->d_scale, sizeof(float)), "scale");
-        if (s == FDK_OK) ck(cudaMemcpy(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice), "scale");
+        if (s == FDK_OK)
+            ck(cudaMemcpyAsync(h->d_scale, &k, sizeof(float), cudaMemcpyHostToDevice, h->compute), "scale");
         // the filter, chosen by measurement: on the C3/C4 workloads the split-FP16 tensor-core
         // GEMM (fdk_toeplitz_*) matches the FFT filter's accuracy (rel-L2 2e-4, the FP16 output
         // rounding) in 0.61x (C3) / 0.67x (C4) of its time.  The FFT filter remains where the GEMM
@@ -315,6 +329,7 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
                           precision, device);
         if (s == FDK_OK && h->d_scale) s = fdk_bp_set_acc_scale_internal(h->bp, h->d_scale);
     }
+    if (s == FDK_OK) s = wait_stream(h->compute, h->sync_ev[0], "fdk_recon_create");  // set-up copies landed
     if (s != FDK_OK) {
         recon_release(h);
         return s;
@@ -348,7 +363,7 @@ int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t
         last = h->raw_ready[k];
     }
     // the caller may reuse host_views once its last copy has landed
-    if (last) FDK_CUDA(cudaEventSynchronize(last));
+    if (last) FDK_TRY(wait_event(last, "view copy"));
     return FDK_OK;
     FDK_ABI_END
 }
@@ -392,7 +407,7 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
     int b = 0;
     for (long long c = 0; c < n; c += cap, b ^= 1) {
         const int m = (int)std::min<long long>(cap, n - c);
-        FDK_CUDA(cudaEventSynchronize(h->stage_free[b]));  // staging b's previous copy has landed
+        FDK_TRY(wait_event(h->stage_free[b], "staging copy"));  // staging b's previous copy has landed
         FDK_TRY(read_views(folder, nu, nv, first + c, m, step, start, h->h_stage[b], threads));
         const int k = h->slot;
         h->slot = (k + 1) % (int)h->d_raw.size();
@@ -458,8 +473,9 @@ int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms) {
                                             (long long)limit);
         std::this_thread::sleep_for(std::chrono::microseconds(200));
     }
-    unsigned int ovf = 0;
-    FDK_CUDA(cudaMemcpy(&ovf, h->d_overflow, sizeof(ovf), cudaMemcpyDeviceToHost));
+    FDK_CUDA(cudaMemcpyAsync(h->h_word, h->d_overflow, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->compute));
+    FDK_TRY(wait_stream(h->compute, h->sync_ev[0], "overflow flag"));
+    const unsigned int ovf = *h->h_word;
     if (ovf)
         return fail(FDK_ERR_DEVICE_CHECK, "filtered views exceeded the FP16 range; use FDK_BP_FP32 for this data");
     if (h->tpz) FDK_TRY(fdk_toeplitz_check(h->tpz));
@@ -479,6 +495,15 @@ int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size) {
     // band by band, overlapping the last batch's backprojection; then the filter checks
     FDK_TRY(fdk_bp_get_volume(h->bp, host_vol, size));
     return fdk_recon_sync(h, 0);
+    FDK_ABI_END
+}
+
+int fdk_recon_sample(fdk_recon *h, const int32_t *host_xyz, int64_t n, float *host_out) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h != nullptr, "NULL handle");
+    FDK_TRY(fdk_recon_sync(h, 0));
+    return fdk_bp_sample(h->bp, host_xyz, n, host_out);
     FDK_ABI_END
 }
 
@@ -509,10 +534,10 @@ int fdk_recon_reset(fdk_recon *h) {
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_CUDA(cudaStreamSynchronize(h->copy));
-    FDK_CUDA(cudaStreamSynchronize(h->compute));
+    FDK_TRY(wait_stream(h->copy, h->sync_ev[1], "fdk_recon_reset"));
+    FDK_TRY(wait_stream(h->compute, h->sync_ev[0], "fdk_recon_reset"));
     FDK_TRY(collect_filter_timers(h));
-    FDK_CUDA(cudaMemset(h->d_overflow, 0, sizeof(unsigned int)));
+    FDK_CUDA(cudaMemsetAsync(h->d_overflow, 0, sizeof(unsigned int), h->compute));
     h->filter_ms = 0;
     h->views = 0;
     h->filter_launches = 0;

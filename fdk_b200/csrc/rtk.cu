@@ -447,7 +447,7 @@ int fdk_rtk_reconstruct_conebeam(const int32_t proj_size[3], const int32_t vol_s
     cudaError_t e = cudaMemcpy(d_proj, proj, bytes, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         s = rtk_launch(proj_size, vol_size, matrices, dev_vol_in, dev_vol_out, d_proj, nullptr);
-        if (s == FDK_OK) e = cudaDeviceSynchronize();
+        if (s == FDK_OK) e = cudaStreamSynchronize(cudaStreamLegacy);  // synchronous, as the reference
     }
     if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, "CUDA_reconstruct_conebeam", __FILE__, __LINE__);
     if (s == FDK_OK) s = rtk_check_device_error();
@@ -472,7 +472,11 @@ int fdk_rtk_backproject_device(const int32_t proj_size[3], const int32_t vol_siz
 int fdk_rtk_sync(void *stream) {
     FDK_ABI_BEGIN
     clear_error();
-    FDK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    cudaEvent_t ev = nullptr;
+    FDK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    const int s = wait_stream((cudaStream_t)stream, ev, "fdk_rtk_sync");  // bounded
+    cudaEventDestroy(ev);
+    FDK_TRY(s);
     return rtk_check_device_error();
     FDK_ABI_END
 }

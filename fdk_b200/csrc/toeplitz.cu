@@ -524,15 +524,20 @@ int fdk_toeplitz_create(fdk_toeplitz **out, const float *cos_table, const double
     auto step = [&](cudaError_t e, const char *what) {
         if (s == FDK_OK && e != cudaSuccess) s = cuda_status(e, what, __FILE__, __LINE__);
     };
-    step(cudaMalloc(&h->d_M, m16.size() * 2), "cudaMalloc M");
-    if (s == FDK_OK) step(cudaMemcpy(h->d_M, m16.data(), m16.size() * 2, cudaMemcpyHostToDevice), "copy M");
+    SetupStream ss;  // set-up copies: a private stream, waited for below (no device-wide sync)
+    s = ss.open();
+    if (s == FDK_OK) step(cudaMalloc(&h->d_M, m16.size() * 2), "cudaMalloc M");
+    if (s == FDK_OK)
+        step(cudaMemcpyAsync(h->d_M, m16.data(), m16.size() * 2, cudaMemcpyHostToDevice, ss.st), "copy M");
     if (s == FDK_OK && cos_table) {
         step(cudaMalloc(&h->d_cos, sizeof(float) * nu * nv), "cudaMalloc cos");
         if (s == FDK_OK)
-            step(cudaMemcpy(h->d_cos, cos_table, sizeof(float) * nu * nv, cudaMemcpyHostToDevice), "copy cos");
+            step(cudaMemcpyAsync(h->d_cos, cos_table, sizeof(float) * nu * nv, cudaMemcpyHostToDevice, ss.st),
+                 "copy cos");
     }
     if (s == FDK_OK) step(cudaMalloc(&h->d_err, 2 * sizeof(unsigned)), "cudaMalloc err");
-    if (s == FDK_OK) step(cudaMemset(h->d_err, 0, 2 * sizeof(unsigned)), "memset err");
+    if (s == FDK_OK) step(cudaMemsetAsync(h->d_err, 0, 2 * sizeof(unsigned), ss.st), "memset err");
+    if (s == FDK_OK) s = ss.finish("fdk_toeplitz_create");
     if (s == FDK_OK) step(cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device), "SM count");
     if (s == FDK_OK)
         step(cudaFuncSetAttribute(tpz::toeplitz_gemm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -80,6 +80,14 @@ class Reconstructor:
         p = self.param
         check(lib().fdk_recon_get_volume(self._h, host_ptr, p.nx * p.ny * self.depth))
 
+    def sample(self, xyz: np.ndarray) -> np.ndarray:
+        """Values at voxels xyz ((n, 3) int (x, y, z) of the whole volume) after a sync; voxels
+        outside the slab pair read NaN.  Reads n values instead of the whole volume."""
+        xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+        out = np.empty(len(xyz), np.float32)
+        check(lib().fdk_recon_sample(self._h, xyz.ctypes.data, len(xyz), out.ctypes.data))
+        return out
+
     def stats(self):
         bp, fl, n = C.c_double(), C.c_double(), C.c_int64()
         check(lib().fdk_recon_stats(self._h, C.byref(bp), C.byref(fl), C.byref(n)))

@@ -170,8 +170,10 @@ int fdk_filter_row_real32(const fdk_dataref *src, fdk_dataref *dst, const fdk_da
  * every GPU using the library holds until the process exits; filter->width (W) must be at most
  * 4096, larger W is rejected with FDK_ERR_INVALID_ARG.  All calls share the array and each call
  * rewrites the entries it uses; calls that overlap on one GPU (from several host threads) race
- * and must be serialised by the caller.  The first call on a device looks up the array's address;
- * make that first call before starting any stream capture.  Synchronous, like the original. */
+ * and must be serialised by the caller.  Each call looks up the array's address on the current
+ * device; the first call on a device also loads the library's device code there, so make that
+ * first call before starting any stream capture.  Synchronous, like the original: the kernels run
+ * on the legacy default stream and the call returns once that stream has finished them. */
 int fdk_filter_row_real32_noalloc(const fdk_dataref *src, fdk_dataref *dst, const fdk_dataref *filter);
 
 /* ---- backprojection: BackProjectionFDK (cudaBP/backprojection.cuh:246-271) -- */
@@ -215,6 +217,11 @@ int fdk_bp_bp_device(fdk_bp *h, const void *dev_proj, int32_t layout, const floa
 int fdk_bp_get_volume(fdk_bp *h, float *host_vol, int64_t size);
 /* Device pointer of the internal volume ([x][y][zs], zs fastest) and its size in floats. */
 int fdk_bp_volume_device(fdk_bp *h, float **dev_vol, int64_t *count);
+/* No counterpart in the reference (accuracy checks of volumes too large to read back whole).
+ * Values of n listed voxels, host_xyz = n triples (x, y, z) of whole-volume indices, into
+ * host_out (n floats); voxels outside the handle's boxes read NaN.  Waits (bounded) for the
+ * handle's launches first; MIXED folds its compensation term. */
+int fdk_bp_sample(fdk_bp *h, const int32_t *host_xyz, int64_t n, float *host_out);
 /* nBpCount, fKernelTime (cudaBP/backprojection.cuh:130, 265): views backprojected and the summed
  * kernel time in ms (events on the handle's stream). */
 int fdk_bp_stats(fdk_bp *h, int64_t *bp_count, double *kernel_ms);
@@ -287,6 +294,9 @@ int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
  * Implies fdk_recon_sync.  Large volumes are backprojected in z bands; each band is copied out
  * as soon as the last batch has finished it, so most of the copy overlaps that batch. */
 int fdk_recon_get_volume(fdk_recon *h, float *host_vol, int64_t size);
+/* fdk_bp_sample on the reconstructor's volume, after fdk_recon_sync (no counterpart in the
+ * reference): n voxels (x, y, z) of the whole volume; voxels outside the slab pair read NaN. */
+int fdk_recon_sample(fdk_recon *h, const int32_t *host_xyz, int64_t n, float *host_out);
 /* Timing: total BP kernel ms, total filter kernel ms, views done. */
 int fdk_recon_stats(fdk_recon *h, double *bp_ms, double *filter_ms, int64_t *views);
 /* Kernel launches (filter and backprojection) since creation or the last reset. */

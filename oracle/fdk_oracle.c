@@ -371,6 +371,125 @@ void orc_bp_f64(double *vol, const long top[6], long depth_bottom, long nz,
     }
 }
 
+/* ------------------------------------------------------------------------- */
+/* FP64 FDK at sampled voxels (accuracy yardstick at full size)                */
+/* ------------------------------------------------------------------------- */
+
+/* In-place radix-2 FFT of length W with a precomputed table tw[k] = exp(-2 pi i k / W),
+ * k < W/2 (the inverse uses the conjugates and is unscaled). */
+static void fft64_tab(double complex *x, int W, const double complex *tw, int inverse)
+{
+    for (int i = 1, j = 0; i < W; i++) {
+        int bit = W >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) { double complex t = x[i]; x[i] = x[j]; x[j] = t; }
+    }
+    for (int len = 2; len <= W; len <<= 1) {
+        const int step = W / len;
+        for (int i = 0; i < W; i += len)
+            for (int k = 0; k < len / 2; k++) {
+                const double complex w = inverse ? conj(tw[k * step]) : tw[k * step];
+                const double complex a = x[i + k], b = x[i + k + len / 2] * w;
+                x[i + k] = a + b;
+                x[i + k + len / 2] = a - b;
+            }
+    }
+}
+
+/* FDK in double precision at a list of voxels.  Backprojection is independent per voxel, so a
+ * full-size reconstruction can be checked on sampled voxels and whole slices without holding
+ * the volume.  For each of the n raw views (nv rows of nu, FP32, consecutive, with their FP64
+ * 3x4 matrices):
+ *   - the row filter of FilterEngine::Filtering (Filterlib/FilterLib.h:167-196), as
+ *     orc_filter_view: optional cosine weight, edge pads of the mean of pad_n samples at offset
+ *     (W-nu)>>1, FFT x H, inverse FFT / W, crop -- kept in double (two rows per complex
+ *     transform: H is real and even, so the real and imaginary parts filter independently);
+ *   - for every listed voxel (x, y, z) (vox: int32 triples, volume index coordinates) the
+ *     sample of orc_bp_f64 / cudaFdkBP (cudaBP/backprojectionFDK.cu:80-114): Z = 1/(m2.X),
+ *     U = (m0.X) Z, v = (m1.X) Z, bilinear over (U, v) with SUBPIXEL's bounds (0 <= v < nv-1,
+ *     0 <= U < nu-1; backprojectionFDK.cu:18), times Z^2, added to out[i] (out accumulates, so
+ *     views may come in several calls).
+ * edge (optional, n_vox bytes) is set to 1 where some view puts the voxel within 1e-3 px of a
+ * border of the bounds rule (the knife-edge voxels, where the rule is discontinuous and a
+ * different FP32 rounding switches a whole sample on or off).  Returns 0, or < 0 on bad input. */
+int orc_fdk_sampled(const float *views, int n, long nu, long nv, const float *cos_table, const double *H, int W,
+                    int pad_n, const double *mats, const int32_t *vox, long n_vox, double *out, uint8_t *edge)
+{
+    if (W < nu || pad_n < 1 || pad_n > nu || n < 0 || n_vox < 0) return -1;
+    double complex *tw = (double complex *)malloc(sizeof(double complex) * (W / 2 > 0 ? W / 2 : 1));
+    double *fd = (double *)malloc(sizeof(double) * nu * nv);
+    if (!tw || !fd) { free(tw); free(fd); return -2; }
+    for (int k = 0; k < W / 2; k++) tw[k] = cos(-2 * M_PI * k / W) + I * sin(-2 * M_PI * k / W);
+    const long off = (W - nu) >> 1;
+    const long pairs = (nv + 1) / 2;
+    for (int s = 0; s < n; s++) {
+        const float *src = views + (long)s * nu * nv;
+#pragma omp parallel
+        {
+            double complex *buf = (double complex *)malloc(sizeof(double complex) * W);
+            double *row = (double *)malloc(sizeof(double) * 2 * nu);
+#pragma omp for schedule(static)
+            for (long q = 0; q < pairs; q++) {
+                const long r0 = 2 * q, r1 = 2 * q + 1 < nv ? 2 * q + 1 : -1;
+                double pad[4] = {0, 0, 0, 0};
+                for (int h = 0; h < 2; h++) {
+                    const long r = h ? r1 : r0;
+                    double *rw = row + h * nu;
+                    for (long c = 0; c < nu; c++) {
+                        double p = r >= 0 ? src[r * nu + c] : 0.0;
+                        if (cos_table && r >= 0) p *= (double)cos_table[r * nu + c];
+                        rw[c] = p;
+                    }
+                    double lv = 0, rv = 0;
+                    for (int k = 0; k < pad_n; k++) { lv += rw[k]; rv += rw[nu - 1 - k]; }
+                    pad[2 * h] = lv / pad_n;
+                    pad[2 * h + 1] = rv / pad_n;
+                }
+                for (long k = 0; k < W; k++) {
+                    double a, b;
+                    if (k < off) { a = pad[0]; b = pad[2]; }
+                    else if (k < off + nu) { a = row[k - off]; b = row[nu + k - off]; }
+                    else { a = pad[1]; b = pad[3]; }
+                    buf[k] = a + I * b;
+                }
+                fft64_tab(buf, W, tw, 0);
+                for (long k = 0; k < W; k++) buf[k] *= H[k];
+                fft64_tab(buf, W, tw, 1);
+                for (long c = 0; c < nu; c++) {
+                    fd[c * nv + r0] = creal(buf[off + c]) / W;
+                    if (r1 >= 0) fd[c * nv + r1] = cimag(buf[off + c]) / W;
+                }
+            }
+            free(buf);
+            free(row);
+        }
+        const double *m = mats + 12 * (long)s;
+#pragma omp parallel for schedule(static)
+        for (long i = 0; i < n_vox; i++) {
+            const double x = vox[3 * i], y = vox[3 * i + 1], z = vox[3 * i + 2];
+            const double Z = 1.0 / (m[8] * x + m[9] * y + m[10] * z + m[11]);
+            const double U = (m[0] * x + m[1] * y + m[2] * z + m[3]) * Z;
+            const double v = (m[4] * x + m[5] * y + m[6] * z + m[7]) * Z;
+            if (edge) {
+                const double e = 1e-3;
+                if (fabs(v) < e || fabs(v - (nv - 1)) < e || fabs(U) < e || fabs(U - (nu - 1)) < e) edge[i] = 1;
+            }
+            if (v >= 0 && v < nv - 1 && U >= 0 && U < nu - 1) {
+                const double fv = floor(v), fu = floor(U);
+                const double a = v - fv, b = U - fu;
+                const double *p0 = fd + (long)fu * nv + (long)fv;
+                const double *p1 = p0 + nv;
+                const double val = (p0[0] * (1 - a) + p0[1] * a) * (1 - b) + (p1[0] * (1 - a) + p1[1] * a) * b;
+                out[i] += val * Z * Z;
+            }
+        }
+    }
+    free(tw);
+    free(fd);
+    return 0;
+}
+
 /* GetVolumeData (cudaBP/backprojectionFDK.cu:278-302 with kernelTransformVolume
  * :131-148): [x][y][zs] -> [zs][y][x] (x fastest).  zs keeps the storage order
  * (top slab ascending, then bottom slab ascending). */

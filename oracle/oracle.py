@@ -67,6 +67,10 @@ def lib():
                                            C.c_double, C.c_double, C.c_double, _f32p]
         L.orc_forward_project.argtypes = ([_f32p] + [C.c_long] * 3 + [C.c_float] * 3 + [C.c_long] * 2 +
                                           [C.c_float] * 4 + [C.c_double, _f32p])
+        L.orc_fdk_sampled.argtypes = [_f32p, C.c_int, C.c_long, C.c_long, C.c_void_p, _f64p, C.c_int, C.c_int,
+                                      _f64p, np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS"), C.c_long,
+                                      _f64p, C.c_void_p]
+        L.orc_fdk_sampled.restype = C.c_int
         _lib = L
     return _lib
 
@@ -143,6 +147,49 @@ def bp_f64(vol: np.ndarray, top, depth_bottom: int, nz: int, proj: np.ndarray,
     n, height, width = proj.shape
     lib().orc_bp_f64(vol, _lp6(*top), depth_bottom, nz, np.ascontiguousarray(proj, np.float32),
                      width, height, np.ascontiguousarray(mats, np.float64).reshape(-1), n)
+
+
+class SampledFDK:
+    """FP64 FDK at a fixed list of voxels (orc_fdk_sampled), fed views in any number of calls.
+
+    vox: (n, 3) int array of voxel indices (x, y, z).  add(views, first) filters the raw views
+    first .. first+len(views)-1 (FP32, (n, nv, nu)) in double and accumulates their samples;
+    values holds the FP64 reconstruction at the voxels, edge marks the knife-edge voxels."""
+
+    def __init__(self, g, vox: np.ndarray, pad_n: int = 4):
+        self.g = g
+        self.vox = np.ascontiguousarray(vox, np.int32).reshape(-1, 3)
+        self.values = np.zeros(len(self.vox), np.float64)
+        self.edge = np.zeros(len(self.vox), np.uint8)
+        self.H = filter_design(g.str_filter, g.nu)
+        self.cos = cos_table(g)
+        self.mats = proj_matrices(g)
+        self.pad_n = pad_n
+
+    def add(self, views: np.ndarray, first: int) -> None:
+        views = np.ascontiguousarray(views, np.float32)
+        n = views.shape[0]
+        mats = np.ascontiguousarray(self.mats[first:first + n])
+        r = lib().orc_fdk_sampled(views.reshape(-1), n, self.g.nu, self.g.nv, self.cos.ctypes.data, self.H,
+                                  len(self.H), self.pad_n, mats.reshape(-1), self.vox.reshape(-1), len(self.vox),
+                                  self.values, self.edge.ctypes.data)
+        assert r == 0, r
+
+
+def sample_voxels(nx: int, ny: int, nz: int, n_random: int, seed: int, slices: bool = True) -> np.ndarray:
+    """Voxel list for a sampled check: n_random seeded uniform voxels, plus (slices) every voxel
+    of the central x, y and z slices.  (n, 3) int32 (x, y, z)."""
+    rng = np.random.default_rng(seed)
+    parts = [np.stack([rng.integers(0, nx, n_random), rng.integers(0, ny, n_random),
+                       rng.integers(0, nz, n_random)], 1)]
+    if slices:
+        a, b = np.meshgrid(np.arange(ny), np.arange(nz), indexing="ij")
+        parts.append(np.stack([np.full(a.size, nx // 2), a.ravel(), b.ravel()], 1))
+        a, b = np.meshgrid(np.arange(nx), np.arange(nz), indexing="ij")
+        parts.append(np.stack([a.ravel(), np.full(a.size, ny // 2), b.ravel()], 1))
+        a, b = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+        parts.append(np.stack([a.ravel(), b.ravel(), np.full(a.size, nz // 2)], 1))
+    return np.ascontiguousarray(np.concatenate(parts), np.int32)
 
 
 def transform_volume(src: np.ndarray, nxs: int, nys: int, D: int) -> np.ndarray:

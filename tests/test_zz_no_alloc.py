@@ -4,8 +4,10 @@ which may synchronise the device, out of their processing loop).
 
 The test calls the new entry point through the C ABI twice in a row (different sizes, so the
 second call must rebuild the shared tables), each time against the existing allocating entry
-point fdk_filter_row_real32 on the same inputs, within the filter tests' tolerance.  It lives in
-a file of its own that pytest collects last, and passes alone or after the other tests."""
+point fdk_filter_row_real32 on the same inputs, within the filter tests' tolerance.  One more
+case checks the tables it builds on the GPU (twiddles from sincospi, the bit-reversed response)
+against the FP64 oracle's row filter (pad 3, the cuFFT plugin's edge rule).  It lives in a file
+of its own that pytest collects last, and passes alone or after the other tests."""
 import ctypes as C
 
 import numpy as np
@@ -49,6 +51,26 @@ def test_noalloc_matches_allocating_entry_point_twice():
         got, want = _filter_both(nu, nv, views, seed)
         err = float(np.abs(got - want).max() / np.abs(want).max())
         assert err <= TOL, (nu, err)
+
+
+def test_noalloc_matches_the_fp64_oracle_at_w4096():
+    import torch
+
+    from oracle import oracle as O
+
+    p = F.config("c1")
+    p.nu, p.nv = 2048, 16  # W = 4096, the largest table the static array holds
+    H = p.fft_kernel_real
+    rng = np.random.default_rng(11)
+    views = (rng.standard_normal((2, p.nv, p.nu)) * 10).astype(np.float32)
+    src = torch.from_numpy(views).cuda()
+    got = torch.empty_like(src)
+    Hd = torch.from_numpy(H.astype(np.float32)).cuda()
+    assert _run(lib().fdk_filter_row_real32_noalloc, src, got, Hd) == 0, lib().fdk_last_error()
+    torch.cuda.synchronize()
+    want = np.stack([O.filter_view(v, H, None, pad_n=3) for v in views])
+    err = float(np.abs(got.cpu().numpy() - want).max() / np.abs(want).max())
+    assert err <= TOL, err
 
 
 def test_noalloc_rejects_filters_longer_than_the_static_tables():
