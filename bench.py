@@ -3,13 +3,26 @@
 
 One step = one batch of 32 views through the hot path (the workload streams 32-view batches):
 cosine weight + ramp/Hann filter at once, backprojection into the resident volume in batches of
-512 views (16 steps; a full batch runs when the next one starts, the last two at the final
-flush), 128 steps = the whole 4096-view reconstruction.
+512 views (a full batch runs when the next one starts, the last two at the final flush), 128
+steps = the whole 4096-view reconstruction.
 GUPS = nx*ny*nz*views / seconds / 1e9 (the reference's definition, cuFDK/mpiFDK.h:211,
 cudaBP/cudaBP.cpp:68).
 
-  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp32|fp32_exact]
+  python bench.py [--gpus N --steps K --warmup W] [--precision mixed|fp32|fp32_exact] [--config c3]
   python bench.py --impl reference ...   (the reference's own CPU FDK, 3dct, on host cores)
+  python bench.py --kernel bp|filter|rtk|learned ...   (one kernel family on a small case, for
+                                                         ncu captures and tuning sweeps)
+
+Besides `value` (device time, views resident in HBM) and `e2e` (host buffers through
+fdk_recon_push, the volume back to pinned host memory), the line carries:
+  accuracy      the run's views reconstructed at full size in MIXED and FP32, checked against
+                the FP64 oracle at sampled voxels and the central x, y, z slices; FP32 (staged)
+                against the reference kernel's arithmetic (fp32_exact) on a central slab pair
+  plain_fp32    the same timed run in plain FP32
+  reference_gpu the reference's own cudaFdkBP (compiled for sm_100a) on a 2048^2 x 512 slab
+                pair beside ours on the same views
+  cpu_baseline  the reference's CPU FDK (3dct) timed on the host cores, extrapolated per view
+  roofline      the backprojection kernel against its measured shared-memory roofline
 
 Under torchrun (N > 1) each rank reconstructs one mirror slab pair of the volume (DivVolume,
 cuFDK/mpiFDK.h:116-149); every rank filters all views itself, so there is no collective on
@@ -70,64 +83,140 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return parse_clock_lines(self.lines)
 
 
-# --------------------------------------------------------------------------- reference arm
-def ref_cpu_rate(param, n_views: int, seed: int = 3, slab: int | None = None, log=print) -> dict:
-    """Time the reference's own CPU FDK (3dct BackProjection<float>: cosine weight, Bourke FFT
-    filter, SSE backprojection; oracle/_ref/libref_cpu.so) on a z-slab of the workload's
-    geometry and extrapolate to the full volume: per view, t = t_filter + (nz/slab) * t_bp."""
+def parse_clock_lines(lines) -> dict:
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        f = [x.strip() for x in ln.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            mx.append(float(f[2]))
+        except ValueError:
+            continue
+        for n, v in zip(names, f[5:9]):
+            if v.lower().startswith("active"):
+                reasons.add(n)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- reference CPU FDK
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+class RefCpuTimer:
+    """The reference's own CPU FDK (3dct BackProjection<float>: cosine weight, Bourke FFT filter,
+    SSE backprojection; oracle/_ref/libref_cpu.so) on all host cores, timed on z-slabs of the
+    workload's geometry centred in the volume (the same per-voxel work as the whole volume).
+
+    Per view the reference's cost is t(S) = f + b*S for an S-slice slab: f is the filtering and
+    per-view set-up, b one slice of backprojection.  calibrate() times `repeats` passes of the
+    same `views` views at S and at S/2 (medians) and one pass at S/4 as a linearity check; the
+    whole volume then costs f + b*nz per view.  Used by the cpu_baseline leg and by
+    --impl reference alike, so both report the same quantity."""
+
+    def __init__(self, param, views: int = 4, slab: int = 256, seed: int = 3, threads: int = 0):
+        from oracle import oracle as O
+        import copy
+
+        import fdk_b200.phantom as P
+
+        self.O, self.param = O, param
+        self.R = O.RefCPU()
+        self.cores = threads or os.cpu_count() or 1
+        self.n_views = views
+        self.S = min(param.nz, slab)
+        ell = P.phantom_for(param, seed, 30)
+        angles = O.view_angles(param)
+        self.views = np.stack([O.ellipsoid_projection(ell, param, angles[i]) for i in range(views)])
+        self.handles = {}
+        for S in sorted({self.S, max(1, self.S // 2), max(1, self.S // 4)}):
+            sp = copy.copy(param)
+            sp.nz = S
+            self.handles[S] = self.R.fdk_handle(sp, param.str_filter)  # tables and buffers, untimed
+        self.f = self.b = None
+        self.calib = {}
+
+    def run(self, S: int) -> float:
+        """Seconds for one pass of the views through 3dct over an S-slice slab."""
+        t0 = time.perf_counter()
+        self.R.fdk_run(self.handles[S], self.views, 0, threads=self.cores)
+        return time.perf_counter() - t0
+
+    def calibrate(self, repeats: int = 3) -> dict:
+        S, h = self.S, max(1, self.S // 2)
+        self.run(S)  # warm-up (page faults of the slab buffers)
+        tS = [self.run(S) for _ in range(repeats)]
+        th = [self.run(h) for _ in range(repeats)] if h < S else tS
+        mS, mh = statistics.median(tS), statistics.median(th)
+        V = self.n_views
+        if h < S:
+            self.b = max((mS - mh) / V / (S - h), 1e-12)
+            self.f = max(mS / V - self.b * S, 0.0)
+        else:  # the slab is the whole volume
+            self.b, self.f = mS / V / S, 0.0
+        q = max(1, S // 4)
+        t4 = self.run(q) if q < h else None
+        self.calib = {"slab_s": [S, h], "t_pass_s": {str(S): tS, str(h): th}, "f_view_s": self.f,
+                      "b_slice_s": self.b,
+                      "linearity": (None if t4 is None else
+                                    {"slices": q, "measured_s": t4, "predicted_s": V * (self.f + self.b * q)}),
+                      "gups_spread": [self.gups(t, S) for t in (max(tS), min(tS))]}
+        return self.calib
+
+    def gups(self, t_pass: float, S: int) -> float:
+        """Whole-volume GUPS implied by one pass over an S-slice slab taking t_pass seconds."""
+        p = self.param
+        per_view = t_pass / self.n_views
+        if self.f is not None and S < p.nz:
+            per_view *= (self.f + self.b * p.nz) / (self.f + self.b * S)
+        return p.nx * p.ny * p.nz / per_view / 1e9
+
+    def sample_text(self) -> str:
+        p = self.param
+        return (f"{self.n_views} views through 3dct over a {self.S}-slice z-slab of {p.nx}x{p.ny} (median of 3 passes), "
+                f"extrapolated to {p.nz} slices per view as f + b*nz (f, b from slabs of {self.S} and "
+                f"{max(1, self.S // 2)} slices); {self.cores} threads on {cpu_model()}")
+
+    def close(self):
+        for h in self.handles.values():
+            self.R.fdk_destroy(h)
+        self.handles = {}
+
+
+def ref_cpu_full(param, threads: int = 0) -> dict:
+    """The reference's CPU FDK over the whole volume and every view (the small workloads run in
+    full): all views projected, then one timed run of 3dct."""
     from oracle import oracle as O
+
     import fdk_b200.phantom as P
 
-    cores = os.cpu_count() or 1
     R = O.RefCPU()
-    S = slab or max(64, 2 * cores)
-    S = min(S, param.nz)
-    import copy
-
-    sp = copy.copy(param)
-    sp.nz = S
-    sp.nProj = param.nProj
-    ell = P.phantom_for(param, seed, 30)
-    # views of the full-size geometry (the slab sits at the volume centre: same per-voxel cost)
-    views = np.stack([O.ellipsoid_projection(ell, param, a) for a in O.view_angles(param)[:n_views]])
-    # filter alone (cos weight + Bourke filter rows), as inside BackProjection
-    H = O.filter_design(param.str_filter, param.nu)
-    cos = O.cos_table(param)
-    t0 = time.perf_counter()
-    R.filter_rows(H, views[0] * cos * O.angular_ramp_factor(param))
-    t_filter = time.perf_counter() - t0
-    h = R.fdk_handle(sp, param.str_filter)  # Parameter::init and buffers outside the timing
+    cores = threads or os.cpu_count() or 1
+    n_ell = 20 if param.nx <= 512 else 30
+    ell = P.phantom_for(param, 2, n_ell)
+    views = np.stack([O.ellipsoid_projection(ell, param, a) for a in O.view_angles(param)])
+    h = R.fdk_handle(param, param.str_filter)
     try:
         t0 = time.perf_counter()
         R.fdk_run(h, views, 0, threads=cores)
-        t_all = time.perf_counter() - t0
+        t = time.perf_counter() - t0
     finally:
         R.fdk_destroy(h)
-    t_view = t_all / n_views
-    t_bp = max(t_view - t_filter, 1e-9)
-    t_full = t_filter + t_bp * (param.nz / S)
-    gups_full = param.nx * param.ny * param.nz / t_full / 1e9
-    gups_sample = param.nx * param.ny * S / t_view / 1e9
-    return {"value": gups_full, "sample_gups": gups_sample, "cores": cores, "slab": S, "views": n_views,
-            "t_view_s": t_view, "t_filter_s": t_filter, "seconds": t_all}
+    return {"value": param.nx * param.ny * param.nz * param.nProj / t / 1e9, "unit": "GUPS", "seconds": t,
+            "cores": cores, "cpu": cpu_model(), "sample": "whole volume, every view"}
 
 
 def run_reference(args, param, rank: int) -> None:
@@ -137,27 +226,25 @@ def run_reference(args, param, rank: int) -> None:
     if not os.path.exists(ref_lib):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build oracle/_ref absent"}))
         return
-    # calibrate the slab so one step (one view) takes about a second
-    cal = ref_cpu_rate(param, 1)
-    cores = cal["cores"]
-    per_slice = max(cal["t_view_s"] - cal["t_filter_s"], 1e-6) / cal["slab"]
-    S = int(max(cores, min(param.nz, (1.0 - min(cal["t_filter_s"], 0.5)) / per_slice)))
-    S = max(8, (S // 8) * 8)
+    T = RefCpuTimer(param)
+    cal = T.calibrate()
     vals, secs = [], 0.0
     for i in range(args.warmup + args.steps):
-        r = ref_cpu_rate(param, 1, seed=3 + i, slab=S)
+        t = T.run(T.S)
         if i >= args.warmup:
-            vals.append(r["value"])
-            secs += r["seconds"]
-    value = float(np.mean(vals))
-    sample = f"{S}-slice z-slab of {param.nx}x{param.ny}, 1 view per step, extrapolated to {param.nz} slices"
+            vals.append(T.gups(t, T.S))
+            secs += t
+    T.close()
+    value = float(statistics.median(vals))
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
         "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded random ellipsoids, exact line integrals)",
         "config": workload_config(param, args),
-        "cpu_baseline": {"value": value, "unit": "GUPS", "cores": cores, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "GUPS", "cores": T.cores, "kind": "reference",
+                         "sample": "each step: " + T.sample_text(), "spread": [min(vals), max(vals)],
+                         "calibration": cal},
         "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -169,16 +256,18 @@ BATCH = 512  # views per backprojection batch (every 16th step); --bp-batch chan
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
-def count_bp_batches(firsts, n: int, batch: int | None = None) -> int:
-    """Backprojection batches the reconstructor runs for pushes of n views starting at `firsts`
-    (from an empty batch, flushed at the end): one per full batch, per push that does not
-    continue the waiting batch, and the final flush.  A batch is one kernel launch per z band.
-    batch: views per batch (default: BATCH)."""
+def count_bp_batches(firsts, n: int, batch: int | None = None) -> list:
+    """Sizes of the backprojection batches the reconstructor runs for pushes of n views
+    starting at `firsts` (from an empty batch, flushed at the end): one per full batch, per push
+    that does not continue the waiting batch, and the final flush.  A batch is one kernel launch
+    per z band.  batch: views per batch (default: BATCH)."""
     batch = batch or BATCH
-    pending, pf, launches = 0, 0, 0
+    sizes = []
+    pending, pf = 0, 0
     for f in firsts:
         if pending and f != pf + pending:
-            launches, pending = launches + 1, 0
+            sizes.append(pending)
+            pending = 0
         done = 0
         while done < n:
             if pending == 0:
@@ -186,8 +275,11 @@ def count_bp_batches(firsts, n: int, batch: int | None = None) -> int:
             m = min(n - done, batch - pending)
             pending, done = pending + m, done + m
             if pending == batch:
-                launches, pending = launches + 1, 0
-    return launches + (1 if pending else 0)
+                sizes.append(pending)
+                pending = 0
+    if pending:
+        sizes.append(pending)
+    return sizes
 
 
 def workload_config(param, args) -> dict:
@@ -202,7 +294,7 @@ def workload_config(param, args) -> dict:
 
 def read_traffic(name: str, key: str):
     """DRAM bytes recorded from an ncu capture: the value of line '<key>: X' in profiles/<name>.md
-    (e.g. dram_bytes_per_256_view_batch_full), or None."""
+    (e.g. dram_bytes_per_512_view_batch_full), or None."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         txt = open(path).read()
@@ -210,6 +302,115 @@ def read_traffic(name: str, key: str):
         return None
     m = re.search(rf"{key}:\s*([0-9.eE+]+)", txt)
     return float(m.group(1)) if m else None
+
+
+def errors(got: np.ndarray, want: np.ndarray, mask=None) -> dict:
+    got, want = np.asarray(got, np.float64), np.asarray(want, np.float64)
+    out = {"rel_l2": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+           "max_abs_rel": float(np.abs(got - want).max() / np.abs(want).max()), "voxels": int(got.size)}
+    if mask is not None and mask.any():
+        g, w = got[~mask], want[~mask]
+        out["masked"] = {"rel_l2": float(np.linalg.norm(g - w) / np.linalg.norm(w)),
+                         "max_abs_rel": float(np.abs(g - w).max() / np.abs(w).max()),
+                         "excluded_knife_edge_voxels": int(mask.sum())}
+    return out
+
+
+def accuracy_leg(F, param, views, n_views: int, slab, local: int, log) -> dict:
+    """The first n_views views of the scan (the run's views), reconstructed at full size in MIXED
+    and FP32, against the FP64 oracle (checker only) at 1e5 seeded voxels and every voxel of the
+    central x, y and z slices of this rank's slab pair; then FP32 (staged) against the reference
+    kernel's arithmetic (fp32_exact, bit-identical to cudaFdkBP) on a central 2 x 64-slice slab
+    pair.  Knife-edge voxels (projected within 1e-3 px of a detector border in some view, where
+    the reference's bounds rule is discontinuous) are reported unmasked and excluded."""
+    from oracle import oracle as O
+
+    import torch
+
+    t0 = time.perf_counter()
+    vox = O.sample_voxels(param.nx, param.ny, param.nz, 100000, 17)
+    z0, d = slab
+    inside = ((vox[:, 2] >= z0) & (vox[:, 2] < z0 + d)) | ((vox[:, 2] >= param.nz - z0 - d) &
+                                                             (vox[:, 2] < param.nz - z0))
+    vox = np.ascontiguousarray(vox[inside])
+    got = {}
+    for prec in ("mixed", "fp32"):
+        r = F.Reconstructor(param, prec, batch=BATCH, device=local, slab=slab)
+        for c in range(0, n_views, PUSH):
+            r.push_device(views[c:].data_ptr(), c, min(PUSH, n_views - c))
+        got[prec] = r.sample(vox)
+        r.close()
+    S = O.SampledFDK(param, vox)
+    for c in range(0, n_views, 64):
+        m = min(64, n_views - c)
+        S.add(views[c:c + m].cpu().numpy(), c)
+    mask = S.edge.astype(bool)
+    res = {"vs": "fp64 oracle (sampled)", "views": n_views,
+           "voxels": f"{len(vox)}: 1e5 seeded random voxels + the central x, y and z slices (within the slab pair)",
+           "mixed": errors(got["mixed"], S.values, mask), "fp32": errors(got["fp32"], S.values, mask)}
+    # FP32 staged against the reference arithmetic on a central slab pair
+    zc = z0 + max(0, d // 2 - 32) if z0 + d < param.nz // 2 else max(z0, param.nz // 2 - 64)
+    dc = min(64, d)
+    vols = {}
+    for prec in ("fp32", "fp32_exact"):
+        r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else BATCH, device=local, slab=(zc, dc))
+        for c in range(0, n_views, PUSH):
+            r.push_device(views[c:].data_ptr(), c, min(PUSH, n_views - c))
+        vols[prec] = r.volume().astype(np.float64)
+        r.close()
+    res["fp32_vs_fp32_exact"] = {"slab_pair": [zc, dc], **errors(vols["fp32"], vols["fp32_exact"])}
+    res["seconds"] = time.perf_counter() - t0
+    torch.cuda.empty_cache()
+    log(f"accuracy: {res}")
+    return res
+
+
+def reference_gpu_leg(F, param, views, local: int, log) -> dict | None:
+    """The reference's own cudaFdkBP (oracle/_ref/libref_gpu_bp.so, compiled for sm_100a) on the
+    per-GPU ABCI shape: a 2048 x 2048 x (2 x 256) slab pair (its 32-bit voxel offsets stay valid)
+    from 2048^2 views, 32 views per BP() call, next to our three precisions on the same views."""
+    from oracle import oracle as O
+
+    import torch
+
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_gpu_bp.so")):
+        return None
+    n = PUSH
+    zc, dc = param.nz // 2 - 256, 256
+    # filtered views in the reference's transposed layout (nu rows of nv), FP32, from our filter
+    eng = F.FilterEngine(param.cos_sigma, param.fft_kernel_real_f32, pad_edge=4)
+    filt = torch.empty((n, param.nu, param.nv), dtype=torch.float32, device="cuda")
+    eng.run_device(views.data_ptr(), filt.data_ptr(), n, F.LAYOUT_TRANSPOSED, F.DTYPE_F32, 1.0)
+    torch.cuda.synchronize()
+    host = filt.cpu().numpy()
+    del filt
+    mats = param.proj_matrices()[:n]
+    top = [0, 0, zc, param.nx, param.ny, dc]
+    bot = [0, 0, param.nz - zc - dc, param.nx, param.ny, dc]
+    ref = O.RefGPU().time_bp(host, mats, param.nx, param.ny, param.nz, top, bot)
+    upd = param.nx * param.ny * 2 * dc * n
+    out = {"slab_pair": f"{param.nx}x{param.ny}x(2x{dc}) at z {zc}", "views_per_call": n,
+           "reference_kernel_gups": upd / (ref["kernel_ms"] * 1e-3) / 1e9,
+           "reference_bp_call_gups": upd / (ref["call_ms"] * 1e-3) / 1e9,
+           "reference_note": "BP() call = H2D copy of the views + kernel + cudaDeviceSynchronize (stock path)"}
+    ours = {}
+    for prec in ("fp32_exact", "fp32", "mixed"):
+        nv = 128 if prec != "fp32_exact" else 32 * 4
+        r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else 128, device=local, slab=(zc, dc))
+        r.push_device(views.data_ptr(), 0, 32)  # warm-up
+        r.sync()
+        r.reset()
+        for c in range(0, nv, 32):
+            r.push_device(views[c % views.shape[0]:].data_ptr(), c, 32)
+        r.sync()
+        st = r.stats()
+        ours[prec] = param.nx * param.ny * 2 * dc * nv / (st["bp_ms"] * 1e-3) / 1e9
+        r.close()
+    out["ours_kernel_gups"] = ours
+    out["ratio_over_reference_kernel"] = {k: v / out["reference_kernel_gups"] for k, v in ours.items()}
+    torch.cuda.empty_cache()
+    log(f"reference_gpu: {out}")
+    return out
 
 
 def run_ours(args, param, rank: int, world: int, local: int) -> None:
@@ -294,48 +495,38 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     r, ms, bp_ms, flt_ms, n_launches = timed_device_run(args.precision, args.steps, args.warmup)
     filter_kind = r.filter_kind
     clk = clocks.stop()
+    r.close()
+    del r
+    torch.cuda.empty_cache()
     ms_max = allmax(ms)
-    n_bp_batches = count_bp_batches([batch_of(b)[1] for b in range(args.warmup, args.warmup + args.steps)], B)
+    batch_sizes = count_bp_batches([batch_of(b)[1] for b in range(args.warmup, args.warmup + args.steps)], B)
     value = upd_step_all * args.steps / (ms_max * 1e-3) / 1e9
     kernel_gups = upd_step_rank * args.steps / (bp_ms * 1e-3) / 1e9
     log(f"{args.precision}: {ms / args.steps:.2f} ms/step, {value:.1f} GUPS (BP kernels {kernel_gups:.1f} GUPS, "
         f"filter {flt_ms / args.steps:.3f} ms/step), clocks {clk}")
 
-    # ---- accuracy at full size: this precision vs FP32 on a 2x64-slice slab pair, 64 views
-    acc = None
-    if not args.no_compare and rank == 0 and args.precision != "fp32":
-        z0 = slab[0] + max(0, slab[1] // 2 - 32)
-        d = min(64, slab[1])
-        vols = {}
-        for prec in (args.precision, "fp32"):
-            ra = F.Reconstructor(param, prec, batch=64, device=local, slab=(z0, d))  # 64 views
-            ra.push_device(views.data_ptr(), 0, min(64, n_dev_views))
-            vols[prec] = ra.volume().astype(np.float64)
-            ra.close()
-        a, b = vols[args.precision], vols["fp32"]
-        acc = {"vs": "fp32 (staged) on a 128-slice slab pair, 64 views",
-               "rel_l2": float(np.linalg.norm(a - b) / np.linalg.norm(b)),
-               "max_abs_rel": float(np.abs(a - b).max() / np.abs(b).max())}
-        log(f"accuracy: {acc}")
-
-    # ---- plain FP32 comparison (same workload, fewer steps)
+    # ---- plain FP32: the same timed run (same steps and warm-up) in FP32
     fp32 = None
     if not args.no_compare and args.precision == "mixed":
-        r.close()
-        del r
-        torch.cuda.empty_cache()
-        ks = max(4, args.steps // 8)
-        r2, ms2, bp2, _, _ = timed_device_run("fp32", ks, 2)
-        v2 = upd_step_all * ks / (allmax(ms2) * 1e-3) / 1e9
-        fp32 = {"value": v2, "unit": "GUPS", "steps": ks, "bp_kernel_gups": upd_step_rank * ks / (bp2 * 1e-3) / 1e9,
-                "speedup_mixed_over_fp32": value / v2}
-        log(f"fp32: {fp32}")
+        r2, ms2, bp2, _, _ = timed_device_run("fp32", args.steps, args.warmup)
         r2.close()
         del r2
-    else:
-        r.close()
-        del r
-    torch.cuda.empty_cache()
+        torch.cuda.empty_cache()
+        v2 = upd_step_all * args.steps / (allmax(ms2) * 1e-3) / 1e9
+        fp32 = {"value": v2, "unit": "GUPS", "steps": args.steps, "warmup": args.warmup,
+                "bp_kernel_gups": upd_step_rank * args.steps / (bp2 * 1e-3) / 1e9,
+                "speedup_mixed_over_fp32": value / v2}
+        log(f"fp32: {fp32}")
+
+    # ---- accuracy at full size against the FP64 oracle (rank 0; the checker, not timed)
+    acc = None
+    if not args.no_compare and rank == 0:
+        acc = accuracy_leg(F, param, views, min(n_dev_views, B * args.steps), slab, local, log)
+
+    # ---- the reference's own GPU backprojector beside ours (rank 0, N = 1)
+    ref_gpu = None
+    if not args.no_compare and rank == 0 and world == 1 and param.nu == 2048 and param.nx == 2048:
+        ref_gpu = reference_gpu_leg(F, param, views, local, log)
 
     # ---- end to end through the public API with host buffers
     e2e = None
@@ -372,8 +563,9 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
                "h2d_bytes_per_step": B * frame * 4,
                "d2h_bytes_per_step": (vol_bytes // args.steps) if host_vol is not None else 4,
                "seconds": te, "host_pool_views": pool,
-               "note": "host views are a pinned pool of the workload's views reused cyclically"
-                       if pool < param.nProj else "all views from pinned host memory"}
+               "note": ("the whole volume is read back once at the end, counted per step; "
+                        + ("host views are a pinned pool of the workload's views reused cyclically"
+                           if pool < param.nProj else "all views from pinned host memory"))}
         log(f"e2e: {e2e}")
         re.close()
 
@@ -381,11 +573,17 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and os.path.exists(
             os.path.join(ROOT, "oracle", "_ref", "libref_cpu.so")):
-        c = ref_cpu_rate(param, 2)
-        cpu = {"value": c["value"], "unit": "GUPS", "cores": c["cores"], "kind": "reference",
-               "sample": f"2 views over a {c['slab']}-slice z-slab of {param.nx}x{param.ny} (3dct CPU FDK incl. "
-                         f"filtering), extrapolated to {param.nz} slices"}
-        log(f"cpu: {c}")
+        if args.cpu_full:
+            c = ref_cpu_full(param)
+            cpu = {**c, "kind": "reference"}
+        else:
+            T = RefCpuTimer(param)
+            cal = T.calibrate()
+            T.close()
+            cpu = {"value": float(statistics.median([T.gups(t, T.S) for t in cal["t_pass_s"][str(T.S)]])),
+                   "unit": "GUPS", "cores": T.cores, "kind": "reference", "sample": T.sample_text(),
+                   "spread": cal["gups_spread"], "calibration": cal}
+        log(f"cpu: {cpu}")
 
     if rank == 0:
         bpu = 8 if args.precision == "mixed" else 16        # algorithmic shared-memory bytes per update
@@ -393,16 +591,17 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         peak_smem = peaks["smem_gbs"] * 1e9 / bpu / 1e9
         peak_fma = peaks["fp32_tflops"] * 1e12 / 2 / fpu / 1e9
         peak = min(peak_smem, peak_fma)
-        hbm_bytes_batch = (param.nx * param.ny * 2 * slab[1] * (16 if args.precision == "mixed" else 8)
-                            + BATCH * frame * (4 if args.precision == "mixed" else 8))
+        vol_rmw = param.nx * param.ny * 2 * slab[1] * (16 if args.precision == "mixed" else 8)
+        view_bytes = frame * (4 if args.precision == "mixed" else 8)
+        views_run = sum(batch_sizes)
+        hbm_bytes = len(batch_sizes) * vol_rmw + views_run * view_bytes   # all batches of the run
         mp = {}
         try:
             mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
             hbm_peak, hbm_src = mp["hbm_gbs"], "measured"
         except Exception:
             hbm_peak, hbm_src = 6650.0, "fallback"
-        bp_batch_ms = bp_ms / n_bp_batches
-        bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / n_bp_batches
+        bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / max(1, len(batch_sizes))
         traffic = read_traffic(f"bp_tma_{args.precision}_c2.md", f"dram_bytes_per_{BATCH}_view_batch_full")
         roofline = {
             "kernel": f"bp_tma_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
@@ -410,14 +609,18 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "bound": "smem" if peak_smem <= peak_fma else "fp32",
             "achieved": kernel_gups, "peak": peak, "unit": "GUPS", "frac": kernel_gups / peak,
             "traffic": traffic,
+            "traffic_unit": f"DRAM bytes per full {BATCH}-view batch (ncu, scaled; see profiles)",
             "peak_source": (f"measured on this GPU by fdk_probe_smem ({peaks['smem_gbs']:.0f} GB/s) / {bpu} B "
                             f"per update and fdk_probe_fma ({peaks['fp32_tflops']:.1f} TFLOP/s) / {fpu} FMA per "
                             "update"),
-            "batch_ms": bp_batch_ms,
-            "batch": f"{BATCH} views over the whole volume, run as {bands:g} launches over z bands",
-            "hbm": {"achieved": hbm_bytes_batch / (bp_batch_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
-                    "frac": hbm_bytes_batch / (bp_batch_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
-                    "algorithmic_bytes_per_batch": hbm_bytes_batch},
+            "batches": batch_sizes,
+            "ms_per_view": bp_ms / views_run,
+            "batch": f"batches of up to {BATCH} views over the whole slab pair, each run as {bands:g} launches "
+                     "over z bands",
+            "hbm": {"achieved": hbm_bytes / (bp_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": hbm_bytes / (bp_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src,
+                    "algorithmic_bytes_of_the_run": hbm_bytes,
+                    "per_batch": "volume (+ compensation) read and written once + its views"},
         }
         out_b = 4 if args.precision == "mixed" else 8
         flt_bytes = B * frame * (4 + out_b)
@@ -450,12 +653,158 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": n_launches,
             "filter": filter_kind,
-            "plain_fp32": fp32, "accuracy": acc,
+            "plain_fp32": fp32, "accuracy": acc, "reference_gpu": ref_gpu,
         }
         print(json.dumps(out), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# --------------------------------------------------------------------------- kernel sub-benches
+def timed(run, reps: int) -> float:
+    import torch
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def kernel_bp(args) -> None:
+    """Backprojection batches through the reconstructor on device-resident views (default: the
+    512^3 / 512^2 geometry, 3 batches of 128 views -- views and volume larger than L2, a few GB
+    on the device, small enough for `ncu --set full -k regex:bp_ -s 1 -c 1`)."""
+    import torch
+
+    import fdk_b200 as F
+    from fdk_b200 import phantom as P
+
+    nb, B = args.batches, args.bp_batch
+    p = F.config(args.config)
+    p.nProj = max(p.nProj, B * nb)  # views over the full circle; more when the run asks for more
+    views = torch.empty((B * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
+    P.project(p, P.phantom_for(p, 2, 20), 0, B * nb, views.data_ptr())
+    r = F.Reconstructor(p, args.precision, batch=B)
+    for b in range(nb):
+        r.push_device(views[B * b:].data_ptr(), B * b, B)
+    r.sync()
+    st = r.stats()
+    st["gups"] = p.nx * p.ny * p.nz * B * nb / (st["bp_ms"] * 1e-3) / 1e9
+    print(json.dumps({"kernel": "bp", "config": args.config, "precision": args.precision, "batch": B,
+                      "batches": nb, **st}), flush=True)
+    r.close()
+
+
+def kernel_filter(args) -> None:
+    """Filter variants on device-resident views (default c4: 1536 x 1024, W = 2048): the batched
+    FFT filter and the tensor-core Toeplitz GEMM (FP16/BF16, plain and split), time per batch of
+    `--bp-batch` views (CUDA events), HBM GB/s of the algorithmic bytes, GEMM TFLOP/s.  Accuracy
+    of each variant against the FP64 oracle is checked in tests/test_gpu_toeplitz.py."""
+    import torch
+
+    import fdk_b200 as F
+    from fdk_b200 import phantom as P
+
+    p = F.config(args.config)
+    batch, reps = args.bp_batch, args.reps
+    only = set(args.variants.split(",")) if args.variants else None
+    keep = lambda name: only is None or name in only  # noqa: E731
+    nu, nv = p.nu, p.nv
+    s = float(1.0 / (p.SOD * p.SOD * p.AngularAndrampFactor))
+    views = torch.empty((batch, nv, nu), dtype=torch.float32, device="cuda")
+    P.project(p, P.phantom_for(p, 4, 20), 0, batch, views.data_ptr())
+    out = torch.empty((batch, nu, nv, 2), dtype=torch.float16, device="cuda")
+    frame = nu * nv
+    W = int(F.lib().fdk_filter_length(nu))
+    res = {"kernel": "filter", "workload": f"{args.config}: {batch} views of {nu}x{nv} per batch, W = {W}",
+           "variants": {}}
+    if keep("fft"):
+        eng = F.FilterEngine(p.cos_sigma, p.fft_kernel_real_f32, pad_edge=4)
+        ms = timed(lambda: eng.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, F.DTYPE_F16, s),
+                   reps)
+        res["variants"]["fft"] = {"ms": ms, "hbm_gbs": batch * frame * 8 / (ms * 1e-3) / 1e9}
+    flops = 2.0 * batch * nv * nu * nu
+    for dt, split in (("f16", False), ("bf16", False), ("f16", True), ("bf16", True)):
+        name = f"toeplitz_{dt}{'_split' if split else ''}"
+        if not keep(name):
+            continue
+        tf = F.ToeplitzFilter(p.cos_sigma, p.fft_kernel_real, 4, dt, in_scale=s, split=split)
+        ms = timed(lambda: tf.run_device(views.data_ptr(), out.data_ptr(), batch, F.LAYOUT_MIRROR, 1.0), reps)
+        tf.check()
+        res["variants"][name] = {"ms": ms, "tflops": (3 if split else 1) * flops / (ms * 1e-3) / 1e12}
+        tf.close()
+    print(json.dumps(res), flush=True)
+
+
+def kernel_rtk(args) -> None:
+    """The RTK drop-in on device-resident views (fdk_rtk_backproject_device): a 512^3 FP32 volume
+    from 32 views of 512^2 (c2 geometry, seeded 20-ellipsoid phantom projected on the GPU), circular
+    matrices and tilted ones (m[2] += 0.02 std(m[0]), m[10] += 1e-3, so u and w depend on z); the
+    staged kernel ("tma") and the L1-gather kernel ("l1", FDK_RTK_KERNEL=l1)."""
+    import torch
+
+    import fdk_b200 as F
+    from fdk_b200.backprojection import rtk_backproject_device, rtk_sync
+    from fdk_b200.phantom import phantom_for, project
+
+    n, W, nviews = 512, 512, 32
+    p = F.config("c2")
+    p.nx = p.ny = p.nz = n
+    p.nu = p.nv = W
+    p.nProj = nviews
+    dev = torch.empty((nviews, W, W), dtype=torch.float32, device="cuda")
+    project(p, phantom_for(p, 2, 20), 0, nviews, dev.data_ptr())
+    vin = torch.zeros((n, n, n), dtype=torch.float32, device="cuda")
+    vout = torch.empty_like(vin)
+    size = (W, W, nviews), (n, n, n)
+    for geo in ("circular", "tilted"):
+        mats = p.proj_matrices(np.float64)
+        if geo == "tilted":
+            mats[:, 2] += 0.02 * mats[:, 0].std()
+            mats[:, 10] += 1e-3
+        mats = mats.astype(np.float32)
+        for kern in (args.variants.split(",") if args.variants else ["tma", "l1"]):
+            if kern == "l1":
+                os.environ["FDK_RTK_KERNEL"] = "l1"
+            else:
+                os.environ.pop("FDK_RTK_KERNEL", None)
+            run = lambda: rtk_backproject_device(*size, mats, vin.data_ptr(), vout.data_ptr(), dev.data_ptr())  # noqa
+            ms = timed(run, args.reps)
+            rtk_sync()
+            print(json.dumps({"kernel": "rtk", "geometry": geo, "variant": kern, "ms": ms,
+                              "gups": n ** 3 * nviews / (ms * 1e-3) / 1e9}), flush=True)
+
+
+def kernel_learned(args) -> None:
+    """The learned-filter training step on the C5 geometry (256^3 volume, 90 views of 256^2): one
+    noisy scan, then --reps forward + loss + gradient passes (network forward, backprojection,
+    volume MSE, backprojection adjoint, network backward); about 0.3 GB on the device."""
+    import torch
+
+    from fdk_b200 import learned as Lr
+
+    pl = Lr.Pipeline()
+    p = pl.p
+    x = torch.empty((p.nProj, p.nv, p.nu), dtype=torch.float32, device=pl.dev)
+    pl.scan(1000, x)
+    w = torch.from_numpy(Lr.init_params()).to(pl.dev)
+    w[-(32 * 9 + 1):] = 0.01
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        pl.truth_of(1000)
+        pl.reconstruct(w, x)
+        e = pl.mse(True)
+        pl.gradient(w, x)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel": "learned", "steps": args.reps,
+                      "ms_per_step": 1e3 * (time.perf_counter() - t0) / args.reps, "mse": e}), flush=True)
 
 
 def main():
@@ -466,18 +815,29 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp32", "fp32_exact"])
-    ap.add_argument("--config", default="c3")
-    ap.add_argument("--bp-batch", type=int, default=BATCH, help="views per backprojection batch")
+    ap.add_argument("--config", default=None, help="c1..c5 (default c3; kernel benches: their own)")
+    ap.add_argument("--bp-batch", type=int, default=None, help="views per backprojection batch")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-compare", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP32, accuracy and reference-GPU legs")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-full", action="store_true", help="time the reference CPU FDK on the whole workload")
+    ap.add_argument("--kernel", choices=["bp", "filter", "rtk", "learned"], default=None)
+    ap.add_argument("--batches", type=int, default=3, help="--kernel bp: batches")
+    ap.add_argument("--reps", type=int, default=3, help="--kernel filter/rtk/learned: timed repetitions")
+    ap.add_argument("--variants", default="", help="--kernel filter/rtk: comma-separated variants")
     args = ap.parse_args()
+    if args.kernel:
+        defaults = {"bp": ("c2", 128), "filter": ("c4", 128), "rtk": ("c2", 32), "learned": ("c5", 90)}
+        args.config = args.config or defaults[args.kernel][0]
+        args.bp_batch = args.bp_batch or defaults[args.kernel][1]
+        {"bp": kernel_bp, "filter": kernel_filter, "rtk": kernel_rtk, "learned": kernel_learned}[args.kernel](args)
+        return
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    BATCH = args.bp_batch
+    BATCH = args.bp_batch or BATCH
     from fdk_b200.geometry import config
 
-    param = config(args.config)
+    param = config(args.config or "c3")
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

@@ -751,5 +751,15 @@ int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layo
     FDK_ABI_END
 }
 
+// The staged kernels' device error word (bounded waits that ran out), read and cleared after
+// the handle's launches have finished.  Internal to the library (recon.cu).
+int fdk_bp_check_internal(fdk_bp *h) {
+    if (!h) return FDK_ERR_INVALID_ARG;
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(collect_timers(h));
+    return check_device_error(h);
+}
+
 // z bands of a batch (1 where the kernel has none).  Internal to the library (recon.cu).
 int fdk_bp_band_count_internal(const fdk_bp *h) { return h ? h->n_bands : 1; }

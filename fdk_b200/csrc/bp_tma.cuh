@@ -100,6 +100,8 @@ struct BpTmaArgs {
     float wscale;
     int tiles_x, tiles_y, tiles_z;
     int tz0;  // first z tile of this launch (a launch may cover a band of z tiles)
+    unsigned long long wait_ns;  // limit of every mbarrier wait (FDK_BP_WAIT_NS, default 10 s)
+    int withhold;  // test switch (FDK_BP_TEST_WITHHOLD): CTA 0 never fills its first stage
 };
 
 template <typename E>
@@ -440,10 +442,11 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
             for (int c = 0; c < n_chunks; c++, it++) {
                 const int s = it % S;
                 const unsigned ph = (unsigned)(it / S) & 1u;
-                if (it >= S && !mbar_wait(empty0 + 8 * s, ph ^ 1u)) {
+                if (it >= S && !mbar_wait(empty0 + 8 * s, ph ^ 1u, a.wait_ns)) {
                     ok = false;
                     break;
                 }
+                if (a.withhold && blockIdx.x == 0 && it == 0) continue;  // the consumers' wait runs out
                 const int view = c * NV + lane;
                 if (lane < NV) {
                     TmaMeta &md = meta[s * NV + lane];
@@ -471,12 +474,13 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
                 __syncwarp();
             }
         }
-        if (!ok) {
-            if (lane == 0) atomicOr(a.err, kErrTimeout);
-            // drain: wait (bounded) for the stages whose copies may still be in flight
-            if (lane == 0)
-                for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(full0 + 8 * (k % S), (unsigned)(k / S) & 1u);
-        }
+        if (!ok && lane == 0) atomicOr(a.err, kErrTimeout);
+        // drain (always): wait, bounded, for the copies of the last stages to land before the CTA
+        // may exit -- consumers that gave up on a wait have left already.  Immediate when the
+        // consumers have waited for these stages themselves.
+        if (lane == 0)
+            for (int k = (it > S ? it - S : 0); k < it; k++)
+                mbar_wait(full0 + 8 * (k % S), (unsigned)(k / S) & 1u, a.wait_ns);
         return;
     }
 
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
         for (int c = 0; c < n_chunks; c++, it++) {
             const int s = it % S;
             const unsigned ph = (unsigned)(it / S) & 1u;
-            if (!mbar_wait(full0 + 8 * s, ph)) {
+            if (!mbar_wait(full0 + 8 * s, ph, a.wait_ns)) {
                 if (lane == 0) atomicOr(a.err, kErrTimeout);
                 return;
             }
@@ -557,6 +561,20 @@ inline int tma_prepare(int &ctas, int device) {
     return FDK_OK;
 }
 
+// Limit of the kernel's mbarrier waits: FDK_BP_WAIT_NS nanoseconds, default 10 s.
+inline unsigned long long bp_wait_ns() {
+    const char *e = getenv("FDK_BP_WAIT_NS");
+    const long long v = e ? atoll(e) : 0;
+    return v > 0 ? (unsigned long long)v : kWaitNs;
+}
+// Test switch FDK_BP_TEST_WITHHOLD=1: CTA 0's producer never fills the first pipeline stage,
+// so its consumers' bounded wait runs out and the launch reports FDK_ERR_DEVICE_CHECK (the
+// timeout path, exercised without a GPU fault).  Off unless the environment sets it.
+inline int bp_test_withhold() {
+    const char *e = getenv("FDK_BP_TEST_WITHHOLD");
+    return (e && atoi(e) == 1) ? 1 : 0;
+}
+
 // Square of the source distance of the volume centre in view 0: keeps f^2 * wscale near 1.
 inline float weight_scale(const float *host_mats, float xc, float yc) {
     const float w = host_mats[8] * xc + host_mats[9] * yc + host_mats[11];
@@ -598,6 +616,8 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     FDK_CHECK_ARG(tz_begin >= 0 && tz_begin < tz_end, "z tiles [%d, %d) outside 0..%d", tz_begin, tz_end, tz_all);
     a.tz0 = tz_begin;
     a.tiles_z = tz_end - tz_begin;
+    a.wait_ns = bp_wait_ns();
+    a.withhold = bp_test_withhold();
     const long long n_tiles = (long long)a.tiles_x * a.tiles_y * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, p.tma_ctas);

@@ -77,6 +77,7 @@ long long fdk_bp_launches_internal(const fdk_bp *h);
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
                                    int32_t n_proj, const float *host_mats, void *stream, int32_t band);
 int fdk_bp_band_count_internal(const fdk_bp *h);
+int fdk_bp_check_internal(fdk_bp *h);
 
 namespace {
 
@@ -479,7 +480,7 @@ int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms) {
     if (ovf)
         return fail(FDK_ERR_DEVICE_CHECK, "filtered views exceeded the FP16 range; use FDK_BP_FP32 for this data");
     if (h->tpz) FDK_TRY(fdk_toeplitz_check(h->tpz));
-    return FDK_OK;
+    return fdk_bp_check_internal(h->bp);  // a backprojection wait that ran out on the device
     FDK_ABI_END
 }
 

@@ -282,12 +282,12 @@ __global__ void __launch_bounds__(rtkt::THREADS, FDK_RTK_MIN_BLOCKS)
                 __syncwarp();
             }
         }
-        if (!ok) {
-            if (lane == 0) atomicOr(&g_rtk_err, kErrTimeout);
-            // drain: wait (bounded) for the stages whose copies may still be in flight
-            if (lane == 0)
-                for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(full0 + 8 * (k % S), (unsigned)(k / S) & 1u);
-        }
+        if (!ok && lane == 0) atomicOr(&g_rtk_err, kErrTimeout);
+        // drain (always): wait, bounded, for the copies of the last stages to land before the CTA
+        // may exit -- consumers that gave up on a wait have left already.  Immediate when the
+        // consumers have waited for these stages themselves.
+        if (lane == 0)
+            for (int k = (it > S ? it - S : 0); k < it; k++) mbar_wait(full0 + 8 * (k % S), (unsigned)(k / S) & 1u);
         return;
     }
 

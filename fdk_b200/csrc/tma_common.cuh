@@ -28,9 +28,9 @@ __device__ __forceinline__ unsigned long long global_ns() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Bounded wait for the phase with the given parity: gives up after kWaitNs of wall time (or
-// kWaitLimit polls); false on timeout.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+// Bounded wait for the phase with the given parity: gives up after limit_ns of wall time
+// (default kWaitNs) or kWaitLimit polls; false on timeout.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned long long limit_ns = kWaitNs) {
     unsigned long long t0 = 0;
     for (long long i = 0; i < kWaitLimit; i++) {
         unsigned ok;
@@ -43,7 +43,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
         if ((i & 255) == 0) {
             const unsigned long long t = global_ns();
             if (i == 0) t0 = t;
-            else if (t - t0 > kWaitNs) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
     return false;

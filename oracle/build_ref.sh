@@ -1,8 +1,8 @@
 #!/usr/bin/env bash
 # Build recipe for the checker's reference binaries (TEST INFRASTRUCTURE ONLY).
 #
-# Compiles the reference's own sources where they lie (FDK_REFERENCE, default
-# /root/reference) through the small extern "C" harnesses in this folder, and
+# Compiles the reference's own sources where they lie (the tree named by the FDK_REFERENCE
+# environment variable) through the small extern "C" harnesses in this folder, and
 # writes every output under oracle/_ref/ (git-ignored; it travels to the GPU box
 # with the rest of the tree).  Nothing from the reference tree is copied into the
 # repository.  The reference's own build system (VisualGDB makefiles) is not used.
@@ -16,10 +16,10 @@
 #     stand-ins for the binding helpers the tested kernels never call.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${FDK_REFERENCE:-/root/reference}"
+REF="${FDK_REFERENCE:-}"
 OUT="$HERE/_ref"
-if [ ! -f "$REF/common/type.h" ]; then
-    echo "build_ref: reference tree not found at $REF; skipping" >&2
+if [ -z "$REF" ] || [ ! -f "$REF/common/type.h" ]; then
+    echo "build_ref: FDK_REFERENCE does not name a reference tree ('$REF'); skipping" >&2
     exit 0
 fi
 NVCC="${NVCC:-/usr/local/cuda/bin/nvcc}"

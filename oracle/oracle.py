@@ -257,8 +257,22 @@ class RefCPU:
                                       [C.c_double] * 4 + [C.c_long, C.c_double, C.c_long, C.c_double,
                                                           C.c_int])
         L.refc_fdk_run.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+        L.refc_forward_projection.argtypes = ([C.c_long] * 3 + [C.c_double] * 3 + [C.c_long] * 2 +
+                                              [C.c_double] * 4 + [C.c_long, C.c_double, C.c_long, C.c_double,
+                                                                  _f32p, C.c_int, _f32p, C.c_int])
+        L.refc_forward_projection.restype = C.c_int
         L.refc_fdk_destroy.argtypes = [C.c_void_p]
         self.L = L
+
+    def forward_projection(self, vol: np.ndarray, g, view: int, threads: int = 0) -> np.ndarray:
+        """3dct ForwardProjection<float> of a [z][y][x] volume for view `view`: (nv, nu)."""
+        out = np.zeros((g.nv, g.nu), np.float32)
+        r = self.L.refc_forward_projection(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz, g.nu, g.nv, g.du, g.dv, g.SID, g.SOD,
+                                           g.direction, g.scan_angle, g.nProj, g.volume_postion_angle,
+                                           np.ascontiguousarray(vol, np.float32).reshape(-1), int(view),
+                                           out.reshape(-1), int(threads))
+        assert r == 0, r
+        return out
 
     def fdk_handle(self, g, ftype="hann"):
         """Persistent reference CPU FDK (tables and buffers built once, outside timing)."""
@@ -318,6 +332,8 @@ class RefGPU:
         self.bp.refg_bp.argtypes = [C.c_void_p, C.c_int, _f32p, C.c_int, C.c_int, _f32p, C.c_int]
         self.bp.refg_bp_get_volume.argtypes = [C.c_void_p, _f32p, C.c_long]
         self.bp.refg_bp_destroy.argtypes = [C.c_void_p]
+        self.bp.refg_bp_kernel_ms.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        self.bp.refg_bp_kernel_ms.restype = C.c_float
         self.flt = C.CDLL(fl)
         self.flt.refg_filter.argtypes = [C.c_void_p] * 4 + [C.c_int] * 4
 
@@ -336,6 +352,32 @@ class RefGPU:
             out = np.zeros(top[3] * top[4] * D, np.float32)
             assert self.bp.refg_bp_get_volume(h, out, out.size) == 0
             return out.reshape(D, top[4], top[3])
+        finally:
+            self.bp.refg_bp_destroy(h)
+
+    def time_bp(self, proj: np.ndarray, mats: np.ndarray, nx, ny, nz, top, bottom, calls: int = 4,
+                launches: int = 4) -> dict:
+        """Speed of the reference's BackProjectionFDK on one GPU: `calls` stock BP(TRANSPOSE = 1)
+        calls of the views (host, (n <= 32, nu, nv) transposed FP32; each call copies them to
+        the device and synchronises, backprojectionFDK.cu:229-276), timed by the host clock,
+        then `launches` launches of its kernel as BP() issues them, timed by CUDA events.
+        Returns ms per call and per launch."""
+        import time
+
+        n, height, width = proj.shape
+        proj = np.ascontiguousarray(proj, np.float32).reshape(-1)
+        mats = np.ascontiguousarray(mats, np.float32).reshape(-1)
+        h = self.bp.refg_bp_create(width, height, 32, nx, ny, nz, _lp6(*top), _lp6(*bottom))
+        assert h, "BackProjectionFDK construction failed"
+        try:
+            assert self.bp.refg_bp(h, 1, proj, width, height, mats, n) == 0  # warm-up
+            t0 = time.perf_counter()
+            for _ in range(calls):
+                assert self.bp.refg_bp(h, 1, proj, width, height, mats, n) == 0
+            call_ms = 1e3 * (time.perf_counter() - t0) / calls
+            kernel_ms = float(self.bp.refg_bp_kernel_ms(h, n, launches))
+            assert kernel_ms > 0, kernel_ms
+            return {"call_ms": call_ms, "kernel_ms": kernel_ms}
         finally:
             self.bp.refg_bp_destroy(h)
 

@@ -8,6 +8,8 @@
 //   refc_filter_rows      filterImageRow         common/type.h:4169-4239 (Bourke FFT, pad 3, double)
 //   refc_cpu_fdk          BackProjection<float>  3dct/3dct.cpp:3-241 (cos*AAF, filter, BP) per view,
 //                         the angle as CTBackProjection forms it (3dct/3dct.cpp:275)
+//   refc_forward_projection  ForwardProjection<float>  3dct/3dct.cpp:430-573, one view, the angle as
+//                         CTForwardProjection forms it (3dct/3dct.cpp:594)
 #define main ref3dct_main_unused
 #include "3dct/3dct.cpp"
 #undef main
@@ -135,4 +137,32 @@ extern "C" void refc_fdk_destroy(void* hv) {
     delete h->vol;
     delete h->cnt;
     delete h;
+}
+
+// ForwardProjection<float> (3dct/3dct.cpp:430-573) of a [z][y][x] FP32 volume for view `view`
+// of the scan: ray-marched sums of the volume's own trilinear samples x min(dx, dy, dz), nv rows
+// of nu into out.  The angle is CTForwardProjection's, -(direction * deg / 180 * PI +
+// volume_postion_angle) (3dct/3dct.cpp:594).  threads <= 0: all.
+extern "C" int refc_forward_projection(long nx, long ny, long nz, double dx, double dy, double dz,
+                                       long nu, long nv, double du, double dv, double sid, double sod,
+                                       long direction, double scan_angle, long nproj, double vpa,
+                                       const float* vol, int view, float* out, int threads) {
+    try {
+        if (threads > 0) omp_set_num_threads(threads);
+        Parameter p;
+        fill_param(p, nx, ny, nz, dx, dy, dz, nu, nv, du, dv, 0, 0, sid, sod, direction, scan_angle,
+                   nproj, vpa, 0);
+        if (view < 0 || view >= p.nProj) return -2;
+        Volume v(nx, ny, nz);
+        memcpy(v.buffer, vol, sizeof(float) * nx * ny * nz);
+        ImageT<float> image((int)nu, (int)nv);
+        ImageT<float> frm((int)nu, (int)nv);
+        image.Clear();
+        const double angle_rad = -(p.direction * p.vec_deg[view] / 180.0 * PI + p.volume_postion_angle);
+        if (!ForwardProjection(p, angle_rad, v, frm.GetFrame(), image)) return -3;
+        memcpy(out, image.buffer, sizeof(float) * nu * nv);
+        return 0;
+    } catch (...) {
+        return -1;
+    }
 }

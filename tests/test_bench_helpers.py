@@ -4,16 +4,18 @@ import bench
 
 def test_batches_of_in_order_pushes():
     # 128 steps of 32 views in order, 128-view batches: one batch per 4 steps
-    assert bench.count_bp_batches([32 * i for i in range(128)], 32, 128) == 32
+    assert bench.count_bp_batches([32 * i for i in range(128)], 32, 128) == [128] * 32
     # a partial last batch is flushed at the end
-    assert bench.count_bp_batches([32 * i for i in range(5)], 32, 128) == 2
+    assert bench.count_bp_batches([32 * i for i in range(5)], 32, 128) == [128, 32]
+    # the driver's 20-step run at 512-view batches: a full batch and a 128-view flush
+    assert bench.count_bp_batches([32 * i for i in range(5, 25)], 32, 512) == [512, 128]
 
 
 def test_batches_break_on_discontinuity():
     # the views restart (the workload wraps around): the waiting batch is backprojected first
-    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128) == 2
+    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128) == [64, 64]
     # a push larger than a batch fills several batches
-    assert bench.count_bp_batches([0], 300, 128) == 3
+    assert bench.count_bp_batches([0], 300, 128) == [128, 128, 44]
 
 
 class _Done:

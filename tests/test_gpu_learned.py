@@ -3,6 +3,7 @@
 finite differences in tests/test_nn_oracle.py), the whole gradient by finite differences, a short
 training that must beat plain FDK, and the committed trained network on held-out scans."""
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -33,6 +34,10 @@ def test_forward_projector_vs_oracle():
     want = np.stack([O.forward_project(vol, p, a) for a in O.view_angles(p)])
     got = out.cpu().numpy()
     assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-4
+    if os.path.exists(os.path.join(O.REF_DIR, "libref_cpu.so")):
+        # and against the reference's own 3dct ForwardProjection (3dct/3dct.cpp:430-573)
+        ref = np.stack([O.RefCPU().forward_projection(vol, p, i) for i in range(6)])
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 1e-4
 
 
 def test_bp_adjoint_dot_product():

@@ -109,3 +109,23 @@ def test_3dct_cpu_fdk_matches_oracle_pipeline():
     core = (xx ** 2 + yy ** 2 < (0.35 * n) ** 2) & (np.abs(zz) < 0.35 * n)
     err = np.linalg.norm((rec - ref)[core]) / np.linalg.norm(ref[core])
     assert err < 2e-4, err
+
+
+@needs_ref
+@pytest.mark.parametrize("n,nu,nv,views", [(48, 56, 40, 6), (64, 64, 64, 9)])
+def test_forward_projector_matches_reference(n, nu, nv, views):
+    """The oracle's ray marcher (orc_forward_project, the learned filter's training-data
+    projector) against the reference's own 3dct ForwardProjection<float> (3dct/3dct.cpp:430-573,
+    angle as CTForwardProjection forms it, :594), built from its sources: same rays, box, step and
+    trilinear samples, FP32 in a different order."""
+    from fdk_b200.phantom import phantom_for
+    from tests.helpers import small_param
+
+    p = small_param(n, nu, nv, views)
+    vol = O.ellipsoid_volume(phantom_for(p, 4, 12), p)
+    R = O.RefCPU()
+    for i, a in enumerate(O.view_angles(p)):
+        ref = R.forward_projection(vol, p, i)
+        got = O.forward_project(vol, p, a)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) <= 2e-5, i
+        assert np.abs(got - ref).max() <= 5e-5 * np.abs(ref).max(), i
