@@ -256,16 +256,30 @@ BATCH = 512  # views per backprojection batch (every 16th step); --bp-batch chan
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
-def count_bp_batches(firsts, n: int, batch: int | None = None) -> list:
+def step_chunks(param, b: int, B: int = PUSH) -> list:
+    """The views of step b as (first, count) chunks: B/4 consecutive views from each quarter of
+    the scan (view v + k N/4, k = 0..3), the read order in which every batch holds whole
+    quarter-turn quadruples (fdk_recon_bp_kernel); all 128 steps of the 4096-view scan read each
+    view once.  Scans whose quarter is not a multiple of B/4 views read B consecutive views."""
+    N = param.nProj
+    c = B // 4
+    if B % 4 == 0 and N % 4 == 0 and (N // 4) % c == 0:
+        q = N // 4
+        base = (b * c) % q
+        return [(base + k * q, c) for k in range(4)]
+    return [((b * B) % N, B)]
+
+
+def count_bp_batches(firsts, n: int, batch: int | None = None, contiguous: bool = False) -> list:
     """Sizes of the backprojection batches the reconstructor runs for pushes of n views
-    starting at `firsts` (from an empty batch, flushed at the end): one per full batch, per push
-    that does not continue the waiting batch, and the final flush.  A batch is one kernel launch
-    per z band.  batch: views per batch (default: BATCH)."""
+    starting at `firsts` (from an empty batch, flushed at the end): one per full batch and the
+    final flush; with `contiguous` (FP32_EXACT) also one per push that does not continue the
+    waiting batch.  batch: views per batch (default: BATCH)."""
     batch = batch or BATCH
     sizes = []
     pending, pf = 0, 0
     for f in firsts:
-        if pending and f != pf + pending:
+        if contiguous and pending and f != pf + pending:
             sizes.append(pending)
             pending = 0
         done = 0
@@ -316,13 +330,14 @@ def errors(got: np.ndarray, want: np.ndarray, mask=None) -> dict:
     return out
 
 
-def accuracy_leg(F, param, views, n_views: int, slab, local: int, log) -> dict:
-    """The first n_views views of the scan (the run's views), reconstructed at full size in MIXED
-    and FP32, against the FP64 oracle (checker only) at 1e5 seeded voxels and every voxel of the
-    central x, y and z slices of this rank's slab pair; then FP32 (staged) against the reference
-    kernel's arithmetic (fp32_exact, bit-identical to cudaFdkBP) on a central 2 x 64-slice slab
-    pair.  Knife-edge voxels (projected within 1e-3 px of a detector border in some view, where
-    the reference's bounds rule is discontinuous) are reported unmasked and excluded."""
+def accuracy_leg(F, param, views, chunks_of, steps: int, slab, local: int, log) -> dict:
+    """The run's views (steps 0..steps-1, chunks_of(b) -> (device pointer, first view, count)),
+    reconstructed at full size in MIXED and FP32, against the FP64 oracle (checker only) at 1e5
+    seeded voxels and every voxel of the central x, y and z slices of this rank's slab pair; then
+    FP32 (staged) against the reference kernel's arithmetic (fp32_exact, bit-identical to
+    cudaFdkBP) on a central 2 x 64-slice slab pair.  Knife-edge voxels (projected within 1e-3 px
+    of a detector border in some view, where the reference's bounds rule is discontinuous) are
+    reported unmasked and excluded."""
     from oracle import oracle as O
 
     import torch
@@ -333,19 +348,23 @@ def accuracy_leg(F, param, views, n_views: int, slab, local: int, log) -> dict:
     inside = ((vox[:, 2] >= z0) & (vox[:, 2] < z0 + d)) | ((vox[:, 2] >= param.nz - z0 - d) &
                                                              (vox[:, 2] < param.nz - z0))
     vox = np.ascontiguousarray(vox[inside])
+    pushes = [c for b in range(steps) for c in chunks_of(b)]
     got = {}
     for prec in ("mixed", "fp32"):
         r = F.Reconstructor(param, prec, batch=BATCH, device=local, slab=slab)
-        for c in range(0, n_views, PUSH):
-            r.push_device(views[c:].data_ptr(), c, min(PUSH, n_views - c))
+        for ptr, first, n in pushes:
+            r.push_device(ptr, first, n)
         got[prec] = r.sample(vox)
+        kind = r.bp_kernel
         r.close()
     S = O.SampledFDK(param, vox)
-    for c in range(0, n_views, 64):
-        m = min(64, n_views - c)
-        S.add(views[c:c + m].cpu().numpy(), c)
+    frame = param.nu * param.nv
+    for ptr, first, n in pushes:
+        i = (ptr - views.data_ptr()) // (4 * frame)
+        S.add(views[i:i + n].cpu().numpy(), first)
     mask = S.edge.astype(bool)
-    res = {"vs": "fp64 oracle (sampled)", "views": n_views,
+    n_views = sum(n for _, _, n in pushes)
+    res = {"vs": "fp64 oracle (sampled)", "views": n_views, "bp_kernel": kind,
            "voxels": f"{len(vox)}: 1e5 seeded random voxels + the central x, y and z slices (within the slab pair)",
            "mixed": errors(got["mixed"], S.values, mask), "fp32": errors(got["fp32"], S.values, mask)}
     # FP32 staged against the reference arithmetic on a central slab pair
@@ -354,8 +373,8 @@ def accuracy_leg(F, param, views, n_views: int, slab, local: int, log) -> dict:
     vols = {}
     for prec in ("fp32", "fp32_exact"):
         r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else BATCH, device=local, slab=(zc, dc))
-        for c in range(0, n_views, PUSH):
-            r.push_device(views[c:].data_ptr(), c, min(PUSH, n_views - c))
+        for ptr, first, n in pushes:
+            r.push_device(ptr, first, n)
         vols[prec] = r.volume().astype(np.float64)
         r.close()
     res["fp32_vs_fp32_exact"] = {"slab_pair": [zc, dc], **errors(vols["fp32"], vols["fp32_exact"])}
@@ -365,10 +384,11 @@ def accuracy_leg(F, param, views, n_views: int, slab, local: int, log) -> dict:
     return res
 
 
-def reference_gpu_leg(F, param, views, local: int, log) -> dict | None:
+def reference_gpu_leg(F, param, views, chunks_of, local: int, log) -> dict | None:
     """The reference's own cudaFdkBP (oracle/_ref/libref_gpu_bp.so, compiled for sm_100a) on the
     per-GPU ABCI shape: a 2048 x 2048 x (2 x 256) slab pair (its 32-bit voxel offsets stay valid)
-    from 2048^2 views, 32 views per BP() call, next to our three precisions on the same views."""
+    from 2048^2 views, 32 views per BP() call, next to our precisions on 128 views of the run
+    (in 128-view batches; MIXED also without the quarter-turn pairing)."""
     from oracle import oracle as O
 
     import torch
@@ -384,6 +404,7 @@ def reference_gpu_leg(F, param, views, local: int, log) -> dict | None:
     torch.cuda.synchronize()
     host = filt.cpu().numpy()
     del filt
+    eng.close()
     mats = param.proj_matrices()[:n]
     top = [0, 0, zc, param.nx, param.ny, dc]
     bot = [0, 0, param.nz - zc - dc, param.nx, param.ny, dc]
@@ -394,20 +415,25 @@ def reference_gpu_leg(F, param, views, local: int, log) -> dict | None:
            "reference_bp_call_gups": upd / (ref["call_ms"] * 1e-3) / 1e9,
            "reference_note": "BP() call = H2D copy of the views + kernel + cudaDeviceSynchronize (stock path)"}
     ours = {}
-    for prec in ("fp32_exact", "fp32", "mixed"):
-        nv = 128 if prec != "fp32_exact" else 32 * 4
+    pushes = [c for b in range(4) for c in chunks_of(b)]  # 128 views
+    for prec, pair in (("fp32_exact", False), ("fp32", True), ("mixed", True), ("mixed", False)):
+        if not pair:
+            os.environ["FDK_BP_SYM"] = "0"
         r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else 128, device=local, slab=(zc, dc))
-        r.push_device(views.data_ptr(), 0, 32)  # warm-up
+        os.environ.pop("FDK_BP_SYM", None)
+        for ptr, first, k in pushes[:4]:  # warm-up
+            r.push_device(ptr, first, k)
         r.sync()
         r.reset()
-        for c in range(0, nv, 32):
-            r.push_device(views[c % views.shape[0]:].data_ptr(), c, 32)
+        for ptr, first, k in pushes:
+            r.push_device(ptr, first, k)
         r.sync()
         st = r.stats()
-        ours[prec] = param.nx * param.ny * 2 * dc * nv / (st["bp_ms"] * 1e-3) / 1e9
+        key = prec if pair or prec == "fp32_exact" else prec + "_unpaired"
+        ours[key] = {"gups": param.nx * param.ny * 2 * dc * 128 / (st["bp_ms"] * 1e-3) / 1e9, "kernel": r.bp_kernel}
         r.close()
-    out["ours_kernel_gups"] = ours
-    out["ratio_over_reference_kernel"] = {k: v / out["reference_kernel_gups"] for k, v in ours.items()}
+    out["ours"] = ours
+    out["ratio_over_reference_kernel"] = {k: v["gups"] / out["reference_kernel_gups"] for k, v in ours.items()}
     torch.cuda.empty_cache()
     log(f"reference_gpu: {out}")
     return out
@@ -445,31 +471,39 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     slab = (int(sp.top.z), int(sp.top.depth))
     B = PUSH
     total_batches = args.warmup + args.steps
-    n_dev_views = min(param.nProj, B * total_batches)
+    pool_steps = min(total_batches, max(1, param.nProj // B))  # distinct steps held in HBM
+    n_dev_views = pool_steps * B
     frame = param.nu * param.nv
     log = (lambda *a: print(*a, file=sys.stderr, flush=True)) if rank == 0 else (lambda *a: None)
 
     peaks = F._lib.probe_peaks(local)
     log(f"probes: {peaks}")
-    # ---- inputs resident in HBM: exact projections of the seeded phantom
+    # ---- inputs resident in HBM: exact projections of the seeded phantom, in step order (step
+    # b's chunks, step_chunks(), one after another; steps beyond the pool reuse it cyclically)
     ell = P.phantom_for(param, 3, 30)
     views = torch.empty((n_dev_views, param.nv, param.nu), dtype=torch.float32, device="cuda")
-    for c in range(0, n_dev_views, 256):
-        n = min(256, n_dev_views - c)
-        P.project(param, ell, c, n, views[c:].data_ptr())
+    for b in range(pool_steps):
+        o = b * B
+        for first, n in step_chunks(param, b):
+            P.project(param, ell, first, n, views[o:].data_ptr())
+            o += n
     torch.cuda.synchronize()
     log(f"generated {n_dev_views} views ({n_dev_views * frame * 4 / GIB:.1f} GiB) in HBM")
 
-    def batch_of(b):
-        first = (b * B) % param.nProj
-        idx = (b * B) % n_dev_views
-        return views[idx:idx + B].data_ptr(), first
+    def chunks_of(b):
+        """Step b's pushes: (device pointer, first view, count)."""
+        o = (b % pool_steps) * B
+        out = []
+        for first, n in step_chunks(param, b):
+            out.append((views[o:].data_ptr(), first, n))
+            o += n
+        return out
 
     def timed_device_run(precision: str, steps: int, warmup: int):
         r = F.Reconstructor(param, precision, batch=BATCH, device=local, slab=slab)
         for b in range(warmup):
-            ptr, first = batch_of(b)
-            r.push_device(ptr, first, B)
+            for ptr, first, n in chunks_of(b):
+                r.push_device(ptr, first, n)
         r.sync()
         st0 = r.stats()
         l0 = r.launch_count
@@ -478,8 +512,8 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for b in range(warmup, warmup + steps):
-            ptr, first = batch_of(b)
-            r.push_device(ptr, first, B)
+            for ptr, first, n in chunks_of(b):
+                r.push_device(ptr, first, n)
         r.flush()  # backproject a last partial batch inside the timed region
         e1.record(stream)
         e1.synchronize()
@@ -494,12 +528,14 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     clocks.start()
     r, ms, bp_ms, flt_ms, n_launches = timed_device_run(args.precision, args.steps, args.warmup)
     filter_kind = r.filter_kind
+    bp_kind = r.bp_kernel
     clk = clocks.stop()
     r.close()
     del r
     torch.cuda.empty_cache()
     ms_max = allmax(ms)
-    batch_sizes = count_bp_batches([batch_of(b)[1] for b in range(args.warmup, args.warmup + args.steps)], B)
+    pushes = [c for b in range(args.warmup, args.warmup + args.steps) for c in step_chunks(param, b)]
+    batch_sizes = count_bp_batches([f for f, _ in pushes], pushes[0][1], contiguous=args.precision == "fp32_exact")
     value = upd_step_all * args.steps / (ms_max * 1e-3) / 1e9
     kernel_gups = upd_step_rank * args.steps / (bp_ms * 1e-3) / 1e9
     log(f"{args.precision}: {ms / args.steps:.2f} ms/step, {value:.1f} GUPS (BP kernels {kernel_gups:.1f} GUPS, "
@@ -521,12 +557,12 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     # ---- accuracy at full size against the FP64 oracle (rank 0; the checker, not timed)
     acc = None
     if not args.no_compare and rank == 0:
-        acc = accuracy_leg(F, param, views, min(n_dev_views, B * args.steps), slab, local, log)
+        acc = accuracy_leg(F, param, views, chunks_of, min(args.steps, pool_steps), slab, local, log)
 
     # ---- the reference's own GPU backprojector beside ours (rank 0, N = 1)
     ref_gpu = None
     if not args.no_compare and rank == 0 and world == 1 and param.nu == 2048 and param.nx == 2048:
-        ref_gpu = reference_gpu_leg(F, param, views, local, log)
+        ref_gpu = reference_gpu_leg(F, param, views, chunks_of, local, log)
 
     # ---- end to end through the public API with host buffers
     e2e = None
@@ -536,7 +572,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         vol_bytes = param.nx * param.ny * 2 * slab[1] * 4
         avail = psutil.virtual_memory().available / max(1, world)
         pool = int(min(n_dev_views, max(64, (avail * 0.6 - vol_bytes) // (frame * 4))))
-        pool = max(B, (pool // B) * B)
+        pool = max(B, (pool // B) * B)  # whole steps of the device pool's step order
         host_views = torch.empty((pool, param.nv, param.nu), dtype=torch.float32, pin_memory=True)
         host_views.copy_(views[:pool])
         host_vol = None
@@ -544,15 +580,25 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             host_vol = torch.empty(param.nx * param.ny * 2 * slab[1], dtype=torch.float32, pin_memory=True)
         del views
         torch.cuda.empty_cache()
+        host_steps = pool // B
+
+        def host_chunks(b):
+            o = (b % host_steps) * B
+            for first, n in step_chunks(param, b % pool_steps):
+                yield host_views[o:].data_ptr(), first, n
+                o += n
+
         re = F.Reconstructor(param, args.precision, batch=BATCH, device=local, slab=slab)
         for b in range(args.warmup):
-            re.push_ptr(host_views[(b * B) % pool:].data_ptr(), (b * B) % param.nProj, B)
+            for ptr, first, n in host_chunks(b):
+                re.push_ptr(ptr, first, n)
         re.sync()
         re.reset()
         barrier()
         t0 = time.perf_counter()
         for b in range(args.steps):
-            re.push_ptr(host_views[(b * B) % pool:].data_ptr(), (b * B) % param.nProj, B)
+            for ptr, first, n in host_chunks(b):
+                re.push_ptr(ptr, first, n)
         if host_vol is not None:
             re.volume_into(host_vol.data_ptr())
         else:
@@ -603,9 +649,10 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             hbm_peak, hbm_src = 6650.0, "fallback"
         bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / max(1, len(batch_sizes))
         traffic = read_traffic(f"bp_tma_{args.precision}_c2.md", f"dram_bytes_per_{BATCH}_view_batch_full")
+        et = '__half2' if args.precision == 'mixed' else 'float2'
         roofline = {
-            "kernel": f"bp_tma_kernel<{'__half2' if args.precision == 'mixed' else 'float2'}>"
-            if args.precision != "fp32_exact" else "bp_exact_kernel",
+            "kernel": {"quarter-turn": f"bp_sym_kernel<{et}> (views paired with their quarter-turn partners)",
+                       "staged": f"bp_tma_kernel<{et}>", "exact": "bp_exact_kernel"}[bp_kind],
             "bound": "smem" if peak_smem <= peak_fma else "fp32",
             "achieved": kernel_gups, "peak": peak, "unit": "GUPS", "frac": kernel_gups / peak,
             "traffic": traffic,
@@ -652,7 +699,9 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "roofline": roofline, "filter_roofline": filter_roof,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": n_launches,
-            "filter": filter_kind,
+            "filter": filter_kind, "bp_kernel": bp_kind,
+            "read_order": ("each step reads 8 consecutive views from each quarter of the scan (views v + k N/4); "
+                           "the 128 steps read every view once"),
             "plain_fp32": fp32, "accuracy": acc, "reference_gpu": ref_gpu,
         }
         print(json.dumps(out), flush=True)

@@ -7,12 +7,16 @@
 // per-view matrices, and the kernel timer.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <string>
 #include <thread>
 #include <vector>
 
 #include "bp_exact.cuh"
 #include "bp_fast.cuh"
+#include "bp_sym.cuh"
 #include "bp_tma.cuh"
 #include "common.h"
 
@@ -200,6 +204,8 @@ struct fdk_bp {
     long long launches = 0;                   // kernel launches since creation or reset
     cudaEvent_t sync_ev[3] = {};              // scratch events of the bounded host waits
     unsigned int *h_err = nullptr;            // pinned host copy of the device error word
+    int sym_rot = 0;                          // quarter-turn kernel: its column map (0: not set up)
+    int sym_ctas = 0;                         // its persistent grid
 };
 
 namespace bpi {
@@ -310,7 +316,10 @@ int check_device_error(fdk_bp *h) {
     if (e) {
         FDK_CUDA(cudaMemsetAsync(h->plan.d_err, 0, sizeof(e), h->stream));
         FDK_TRY(wait_stream(h->stream, h->sync_ev[2], "error word"));
-        return fail(FDK_ERR_DEVICE_CHECK, "backprojection pipeline wait timed out on the device (error word %u)", e);
+        if (e & kErrTimeout)
+            return fail(FDK_ERR_DEVICE_CHECK, "backprojection pipeline wait timed out on the device (error word %u)", e);
+        return fail(FDK_ERR_DEVICE_CHECK, "backprojection: a tile footprint exceeded its shared-memory box and was "
+                                          "skipped (error word %u)", e);
     }
     return FDK_OK;
 }
@@ -375,6 +384,79 @@ int check_circular(const float *mats, int n) {
 }  // namespace bpi
 
 using namespace bpi;
+
+
+namespace {
+
+// Quarter-turn symmetry of the scan (bp_sym.cuh): for every base view p < N/4 and k = 1..3, view
+// p + kN/4 must put column T^k(x, y) where view p puts (x, y), within 1e-3 px, at test voxels
+// spread over the grid; rot is the sign of T (see BpSymArgs::rot).  FP64 arithmetic on the FP32
+// matrices the kernels use.
+bool quarter_turn_holds(const float *mats, int n_proj, int n, int nz, int rot) {
+    const int q = n_proj / 4;
+    const int pts[6][3] = {{0, 0, 0}, {n - 1, 0, nz - 1}, {0, n - 1, nz / 2}, {n - 1, n - 1, 0},
+                           {n / 3, (2 * n) / 3, nz / 3}, {n / 2, n / 5, nz - 1}};
+    auto proj = [&](const float *m, double x, double y, double z, double &u, double &v) {
+        const double w = (double)m[8] * x + (double)m[9] * y + (double)m[10] * z + (double)m[11];
+        u = ((double)m[0] * x + (double)m[1] * y + (double)m[2] * z + (double)m[3]) / w;
+        v = ((double)m[4] * x + (double)m[5] * y + (double)m[6] * z + (double)m[7]) / w;
+    };
+    for (int p = 0; p < q; p++)
+        for (const auto &t : pts) {
+            double u0, v0;
+            proj(mats + 12 * (long long)p, t[0], t[1], t[2], u0, v0);
+            int x = t[0], y = t[1];
+            for (int k = 1; k < 4; k++) {
+                const int nx_ = rot > 0 ? y : n - 1 - y, ny_ = rot > 0 ? n - 1 - x : x;
+                x = nx_;
+                y = ny_;
+                double u, v;
+                proj(mats + 12 * (long long)(p + k * q), x, y, t[2], u, v);
+                if (!(std::fabs(u - u0) <= 1e-3 && std::fabs(v - v0) <= 1e-3)) return false;
+            }
+        }
+    return true;
+}
+
+// Every tile of the quadrant (16 x 16 columns x R slices of the top slab [z0, z0 + nzz)) fits
+// the kernel's BW x BH box in every base view.  The map is linear-fractional, so a tile's
+// extremes sit at its corner columns; the box's u extent is at most umax - umin + 5 and its v
+// extent at most (vmax - vmin) + 7 (floors, margins, 16-byte alignment), and vmax - vmin over a
+// tile (a max minus a min of functions linear in the tile's first slice) is convex along z, so
+// the first and last z tiles bound every z tile.
+bool sym_footprints_fit(const float *mats, int n_proj, int n, int z0, int nzz, int R, int BW, int BH) {
+    const int q = n_proj / 4, half = n / 2, tq = (half + 15) / 16;
+    const int last = z0 + (int)((ceil_div(nzz, R) - 1) * R);
+    for (int p = 0; p < q; p++) {
+        const float *m = mats + 12 * (long long)p;
+        for (int tx = 0; tx < tq; tx++)
+            for (int ty = 0; ty < tq; ty++) {
+                const double xa = tx * 16, xb = std::min(tx * 16 + 16, half) - 1;
+                const double ya = ty * 16, yb = std::min(ty * 16 + 16, half) - 1;
+                double umin = 1e300, umax = -1e300, spread = 0;
+                double vlo[2] = {1e300, 1e300}, vhi[2] = {-1e300, -1e300};
+                for (int c = 0; c < 4; c++) {
+                    const double x = (c & 1) ? xb : xa, y = (c & 2) ? yb : ya;
+                    const double w = (double)m[8] * x + (double)m[9] * y + (double)m[11];
+                    const double U = ((double)m[0] * x + (double)m[1] * y + (double)m[3]) / w;
+                    umin = std::min(umin, U);
+                    umax = std::max(umax, U);
+                    for (int e = 0; e < 2; e++) {
+                        const double zs = e ? last : z0;
+                        const double va = ((double)m[4] * x + (double)m[5] * y + (double)m[6] * zs + (double)m[7]) / w;
+                        const double vb = va + (double)m[6] * (R - 1) / w;
+                        vlo[e] = std::min(vlo[e], std::min(va, vb));
+                        vhi[e] = std::max(vhi[e], std::max(va, vb));
+                    }
+                }
+                for (int e = 0; e < 2; e++) spread = std::max(spread, vhi[e] - vlo[e]);
+                if (umax - umin + 5.01 > BH || spread + 7.01 > BW) return false;
+            }
+    }
+    return true;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -467,16 +549,21 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
     h->band_z[1] = (long long)t.depth;
     if (s == FDK_OK && h->plan.tma_ok && sym) {
         const int R = precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+        // band boundaries fall on whole tiles of both staged kernels (the quarter-turn one too)
+        const int Rs = precision == FDK_BP_MIXED ? SymCfg<__half2>::R : SymCfg<float2>::R;
+        int unit = R;
+        while (unit % Rs) unit += R;
         const long long cols = ceil_div((long long)t.width, 16) * ceil_div((long long)t.height, 16);
         const int tiles_z = (int)ceil_div((long long)t.depth, R);
+        const int units = (int)ceil_div((long long)t.depth, unit);
         const char *cap = getenv("FDK_BP_BANDS");
         const int max_bands = cap ? std::max(1, std::min(kMaxBands, atoi(cap))) : kMaxBands;
-        int nb = std::min(max_bands, tiles_z);
+        int nb = std::min(max_bands, units);
         while (nb > 1 && cols * (tiles_z / nb) < 8ll * h->plan.tma_ctas) nb--;
         h->n_bands = nb;
         for (int k = 0; k <= nb; k++) {
-            h->band_tz[k] = (int)((long long)k * tiles_z / nb);
-            h->band_z[k] = std::min<long long>((long long)h->band_tz[k] * R, (long long)t.depth);
+            h->band_z[k] = std::min<long long>((long long)k * units / nb * unit, (long long)t.depth);
+            h->band_tz[k] = k == nb ? tiles_z : (int)(h->band_z[k] / R);
         }
     }
     for (int k = 0; k < kMaxBands && s == FDK_OK; k++)
@@ -763,3 +850,111 @@ int fdk_bp_check_internal(fdk_bp *h) {
 
 // z bands of a batch (1 where the kernel has none).  Internal to the library (recon.cu).
 int fdk_bp_band_count_internal(const fdk_bp *h) { return h ? h->n_bands : 1; }
+
+// Quarter-turn kernel set-up for device-resident batches (recon.cu): returns in *rot the column
+// map of the scan's quarter-turn symmetry, or 0 where the kernel does not apply (FP32_EXACT, not
+// the whole square grid, n_proj % 4 != 0, matrices without the symmetry, a footprint larger
+// than the box, or FDK_BP_SYM=0).  mats: all n_proj views' matrices (host).  Internal.
+int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot) {
+    FDK_CHECK_ARG(h && mats && rot, "NULL argument");
+    *rot = 0;
+    h->sym_rot = 0;
+    const char *env = getenv("FDK_BP_SYM");
+    if (env && std::string(env) == "0") return FDK_OK;
+    if (h->precision == FDK_BP_FP32_EXACT || !h->plan.tma_ok || !h->sym) return FDK_OK;
+    const BpFastPlan &p = h->plan;
+    if (p.x0 != 0 || p.y0 != 0 || p.nxs != p.nys || p.nxs != h->nx || h->nx != h->ny || (p.nxs & 1) || n_proj % 4)
+        return FDK_OK;
+    if (check_circular(mats, n_proj) != FDK_OK) {
+        clear_error();
+        return FDK_OK;
+    }
+    int r = 0;
+    for (int cand : {1, -1})
+        if (quarter_turn_holds(mats, n_proj, h->nx, h->nz, cand)) {
+            r = cand;
+            break;
+        }
+    if (!r) return FDK_OK;
+    const bool mixed = h->precision == FDK_BP_MIXED;
+    const int R = mixed ? SymCfg<__half2>::R : SymCfg<float2>::R;
+    const int BW = mixed ? SymCfg<__half2>::BW : SymCfg<float2>::BW;
+    const int BH = mixed ? SymCfg<__half2>::BH : SymCfg<float2>::BH;
+    if (!sym_footprints_fit(mats, n_proj, h->nx, p.z0, p.nzz, R, BW, BH)) return FDK_OK;
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(mixed ? sym_prepare<__half2>(h->sym_ctas, h->device) : sym_prepare<float2>(h->sym_ctas, h->device));
+    h->sym_rot = r;
+    *rot = r;
+    return FDK_OK;
+}
+
+// One batch of views held in a device views buffer (n_slots views, any order), for the
+// reconstructor (recon.cu): `n_single` views by (slot, view) through the staged kernel and
+// `n_quad` quarter-turn quadruples (4 slots each, members p, p + N/4, p + N/2, p + 3N/4, and the
+// base view p) through the quarter-turn kernel.  d_mats / host_mats: every view's matrix.
+// band: -1 = every z band, else one.  Internal to the library.
+int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const float *d_mats, const float *host_mats,
+                             const int *s_slot, const int *s_view, int n_single, const int *q_slot,
+                             const int *q_view, int n_quad, void *stream, int band) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h && views && d_mats && host_mats, "NULL argument");
+    FDK_CHECK_ARG(h->precision != FDK_BP_FP32_EXACT && h->plan.tma_ok, "view lists need a staged precision (TMA)");
+    FDK_CHECK_ARG(n_single >= 0 && n_quad >= 0 && n_single + 4 * n_quad > 0, "empty batch");
+    FDK_CHECK_ARG(n_quad == 0 || h->sym_rot != 0, "quadruples without the quarter-turn set-up");
+    FDK_CHECK_ARG(band < h->n_bands, "band %d outside 0..%d", band, h->n_bands - 1);
+    FDK_CHECK_ARG(((uintptr_t)views & 15) == 0, "TMA views must start on a 16-byte boundary");
+    for (int i = 0; i < n_single; i++) FDK_TRY(check_circular(host_mats + 12 * (long long)s_view[i], 1));
+    for (int i = 0; i < n_quad; i++) FDK_TRY(check_circular(host_mats + 12 * (long long)q_view[i], 1));
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool mixed = h->precision == FDK_BP_MIXED;
+    const float *acc_scale = mixed ? h->ext_scale : nullptr;
+    const int kb = band < 0 ? 0 : band, ke = band < 0 ? h->n_bands : band + 1;
+    std::pair<cudaEvent_t, cudaEvent_t> tm;
+    FDK_TRY(take_timer(h, tm));
+    FDK_CUDA(cudaEventRecord(tm.first, st));
+    static thread_local SymQuads sq;
+    static thread_local ViewList vl;
+    for (int k = kb; k < ke; k++) {
+        for (int q0 = 0; q0 < n_quad; q0 += kSymMaxQuads) {
+            const int nq = std::min(kSymMaxQuads, n_quad - q0);
+            for (int i = 0; i < nq; i++) {
+                const int *s4 = q_slot + 4 * (q0 + i);
+                sq.slot[i] = make_int4(s4[0], s4[1], s4[2], s4[3]);
+                sq.view[i] = q_view[q0 + i];
+            }
+            if (mixed)
+                FDK_TRY(bp_sym_launch<__half2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots, d_mats,
+                                               host_mats, sq, nq, h->sym_rot, st, acc_scale, h->band_z[k],
+                                               h->band_z[k + 1]));
+            else
+                FDK_TRY(bp_sym_launch<float2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots, d_mats,
+                                              host_mats, sq, nq, h->sym_rot, st, acc_scale, h->band_z[k],
+                                              h->band_z[k + 1]));
+            h->launches++;
+        }
+        for (int s0 = 0; s0 < n_single; s0 += kMaxListViews) {
+            const int ns = std::min(kMaxListViews, n_single - s0);
+            vl.n = ns;
+            for (int i = 0; i < ns; i++) {
+                vl.slot[i] = s_slot[s0 + i];
+                vl.view[i] = s_view[s0 + i];
+            }
+            if (mixed)
+                FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st, acc_scale,
+                                               h->band_tz[k], h->band_tz[k + 1], &vl, n_slots));
+            else
+                FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st, acc_scale,
+                                              h->band_tz[k], h->band_tz[k + 1], &vl, n_slots));
+            h->launches++;
+        }
+        FDK_CUDA(cudaEventRecord(h->band_done[k], st));
+    }
+    FDK_CUDA(cudaEventRecord(tm.second, st));
+    h->timers.push_back(tm);
+    if (kb == 0) h->bp_count += n_single + 4ll * n_quad;
+    return FDK_OK;
+    FDK_ABI_END
+}

@@ -104,6 +104,16 @@ struct BpTmaArgs {
     int withhold;  // test switch (FDK_BP_TEST_WITHHOLD): CTA 0 never fills its first stage
 };
 
+// Views of one launch taken from a views buffer in any order (kernel parameter): the slot of
+// each (the TMA z coordinate) and its view index (its matrix).  n == 0: views 0..n_proj-1 in
+// slots 0..n_proj-1.
+constexpr int kMaxListViews = 512;
+struct ViewList {
+    int n;
+    int slot[kMaxListViews];
+    int view[kMaxListViews];
+};
+
 template <typename E>
 __host__ __device__ constexpr int tma_box_bytes() {
     return ((TmaCfg<E>::BW * TmaCfg<E>::BH * (int)sizeof(E)) + 127) / 128 * 128;
@@ -404,7 +414,8 @@ template <typename E>
 #ifndef FDK_TMA_MIN_BLOCKS
 #define FDK_TMA_MIN_BLOCKS 2
 #endif
-__global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
+__global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
+    bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ViewList vl, BpTmaArgs a) {
     using C = TmaCfg<E>;
     constexpr int R = C::R, NV = C::NV, S = C::S;
     constexpr int BOX = tma_box_bytes<E>();
@@ -451,8 +462,9 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
                 if (lane < NV) {
                     TmaMeta &md = meta[s * NV + lane];
                     if (view < a.n_proj) {
+                        const float *mg = a.mats + 12 * (long long)(vl.n ? vl.view[view] : view);
 #pragma unroll
-                        for (int q = 0; q < 12; q++) md.m[q] = __ldg(a.mats + 12 * view + q);
+                        for (int q = 0; q < 12; q++) md.m[q] = __ldg(mg + q);
                         tile_box<E>(md.m, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
                     } else {
                         md.staged = 0;
@@ -468,7 +480,8 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
                     for (int l = 0; l < NV; l++) {
                         const TmaMeta &md = meta[s * NV + l];
                         if (c * NV + l < a.n_proj && md.staged)
-                            tma_load_3d(boxes + (s * NV + l) * BOX, &tmap, md.v_lo, md.u_lo, c * NV + l, full0 + 8 * s);
+                            tma_load_3d(boxes + (s * NV + l) * BOX, &tmap, md.v_lo, md.u_lo,
+                                        vl.n ? vl.slot[c * NV + l] : c * NV + l, full0 + 8 * s);
                     }
                 }
                 __syncwarp();
@@ -512,7 +525,8 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS) bp_tma_kernel(const _
                 for (int l = 0; l < NV; l++) {
                     const int view = c * NV + l;
                     if (view >= a.n_proj) break;
-                    column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + view * frame, x, y, zf0, a.nu,
+                    const long long slot = vl.n ? vl.slot[view] : view;
+                    column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + slot * frame, x, y, zf0, a.nu,
                                    a.nv, a.wscale, am, ar);
                 }
             }
@@ -583,14 +597,23 @@ inline float weight_scale(const float *host_mats, float xc, float yc) {
 
 // Backproject n views into the z tiles [tz_begin, tz_end) of R top slices each (with their
 // mirror slices); tz_end < 0 means through the last tile.
+// list (optional): the n views as slots of a buffer of n_slots views and their view indices
+// (matrices d_mats + 12 * view); without it, views and slots 0..n-1.
 template <typename E>
 inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const void *proj, const float *d_mats,
                          const float *host_mats, int n, cudaStream_t st, const float *scale, int tz_begin = 0,
-                         int tz_end = -1) {
+                         int tz_end = -1, const ViewList *list = nullptr, int n_slots = 0) {
     using C = TmaCfg<E>;
     FDK_CHECK_ARG(((uintptr_t)proj & 15) == 0, "TMA views must start on a 16-byte boundary");
+    static thread_local ViewList identity;  // n = 0
+    identity.n = 0;
+    if (list) {
+        FDK_CHECK_ARG(list->n == n && n <= kMaxListViews, "view list of %d entries for %d views", list->n, n);
+        for (int i = 0; i < n; i++)
+            FDK_CHECK_ARG(list->slot[i] >= 0 && list->slot[i] < n_slots, "list entry %d: slot outside the buffer", i);
+    }
     CUtensorMap map;
-    FDK_TRY(encode_views_map<E>(&map, proj, p.nu, p.nv, n));
+    FDK_TRY(encode_views_map<E>(&map, proj, p.nu, p.nv, list ? n_slots : n));
     BpTmaArgs a;
     a.vol = vol;
     a.comp = comp;
@@ -608,7 +631,8 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     a.nys = p.nys;
     a.nzz = p.nzz;
     a.D = p.D;
-    a.wscale = weight_scale(host_mats, p.x0 + 0.5f * (p.nxs - 1), p.y0 + 0.5f * (p.nys - 1));
+    a.wscale = weight_scale(host_mats + (list ? 12 * (long long)list->view[0] : 0), p.x0 + 0.5f * (p.nxs - 1),
+                            p.y0 + 0.5f * (p.nys - 1));
     a.tiles_x = (int)ceil_div(p.nxs, 16);
     a.tiles_y = (int)ceil_div(p.nys, 16);
     const int tz_all = (int)ceil_div(p.nzz, C::R);
@@ -621,7 +645,7 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     const long long n_tiles = (long long)a.tiles_x * a.tiles_y * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, p.tma_ctas);
-    bp_tma_kernel<E><<<grid, 288, tma_smem_bytes<E>(), st>>>(map, a);
+    bp_tma_kernel<E><<<grid, 288, tma_smem_bytes<E>(), st>>>(map, list ? *list : identity, a);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
 }

@@ -17,6 +17,8 @@
 // bounded: fdk_recon_sync polls with a deadline and returns FDK_ERR_TIMEOUT instead of hanging.
 #include <cuda_fp16.h>
 
+#include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstdlib>
 #include <string>
@@ -52,14 +54,16 @@ struct fdk_recon {
     std::vector<cudaEvent_t> raw_ready, raw_free;
     cudaEvent_t done = nullptr;
     int slot = 0;
-    // d_filt[cur] is filling: views pend_first .. pend_first+pending-1.  held: d_filt[cur ^ 1]
-    // holds a full batch (views held_first ..) that is backprojected when the next batch starts,
-    // or together with the filling one at a flush (band-interleaved, see flush_all).
+    // d_filt[cur] is filling: views bviews[cur] (pending of them, in arrival order).  held:
+    // d_filt[cur ^ 1] holds a full batch that is backprojected when the next batch starts, or
+    // together with the filling one at a flush (band-interleaved, see flush_all).  FP32_EXACT
+    // batches hold consecutive views (its kernel reads a contiguous run of matrices); the staged
+    // precisions take views in any order and pair them into quarter-turn quadruples at launch.
     int cur = 0;
     int pending = 0;
-    long long pend_first = 0;
     bool held = false;
-    long long held_first = 0;
+    std::vector<int> bviews[2];
+    int sym_rot = 0;  // quarter-turn kernel's column map (0: not available for this scan)
     double filter_ms = 0;
     long long views = 0;
     long long filter_launches = 0;   // kernel launches of the filter since creation or reset
@@ -72,6 +76,10 @@ struct fdk_recon {
 };
 
 // internal hooks (bp.cu)
+int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot);
+int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const float *d_mats, const float *host_mats,
+                             const int *s_slot, const int *s_view, int n_single, const int *q_slot,
+                             const int *q_view, int n_quad, void *stream, int band);
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
 long long fdk_bp_launches_internal(const fdk_bp *h);
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
@@ -132,22 +140,61 @@ int collect_filter_timers(fdk_recon *h) {
     return FDK_OK;
 }
 
-// Backproject n filtered views of buffer b starting at view `first`: every z band (band -1) or
-// one, on the compute stream.
-int launch_batch(fdk_recon *h, int b, long long first, int n, int band) {
-    return fdk_bp_bp_device_mats_internal(h->bp, h->d_filt[b], h->layout, h->d_mats + 12 * first, n,
-                                          h->mats.data() + 12 * first, h->compute, band);
+// Backproject the n filtered views of buffer b: every z band (band -1) or one, on the compute
+// stream.  FP32_EXACT: one consecutive run.  Staged precisions: the views whose quarter-turn
+// partners (v mod N/4 equal, one from each quarter of the scan) are in the same batch go to the
+// quarter-turn kernel four at a time, the rest to the staged kernel by (slot, view).
+int launch_batch(fdk_recon *h, int b, int n, int band) {
+    const std::vector<int> &vw = h->bviews[b];
+    if (h->precision == FDK_BP_FP32_EXACT) {
+        const long long first = vw[0];
+        return fdk_bp_bp_device_mats_internal(h->bp, h->d_filt[b], h->layout, h->d_mats + 12 * first, n,
+                                              h->mats.data() + 12 * first, h->compute, band);
+    }
+    std::vector<int> s_slot, s_view, q_slot, q_view;
+    if (h->sym_rot) {
+        const int q = (int)(h->g.n_proj / 4);
+        // (orbit, quarter, slot), grouped by orbit: complete quadruples take one slot per quarter
+        std::vector<std::array<int, 3>> e(n);
+        for (int i = 0; i < n; i++) e[i] = {vw[i] % q, vw[i] / q, i};
+        std::sort(e.begin(), e.end());
+        for (size_t i = 0; i < e.size();) {
+            size_t j = i;
+            while (j < e.size() && e[j][0] == e[i][0]) j++;
+            std::vector<int> by_q[4];
+            for (size_t k = i; k < j; k++) by_q[e[k][1]].push_back(e[k][2]);
+            const size_t nq = std::min({by_q[0].size(), by_q[1].size(), by_q[2].size(), by_q[3].size()});
+            for (size_t k = 0; k < nq; k++) {
+                for (int t = 0; t < 4; t++) q_slot.push_back(by_q[t][k]);
+                q_view.push_back(e[i][0]);
+            }
+            for (int t = 0; t < 4; t++)
+                for (size_t k = nq; k < by_q[t].size(); k++) {
+                    s_slot.push_back(by_q[t][k]);
+                    s_view.push_back(vw[by_q[t][k]]);
+                }
+            i = j;
+        }
+    } else {
+        for (int i = 0; i < n; i++) {
+            s_slot.push_back(i);
+            s_view.push_back(vw[i]);
+        }
+    }
+    return fdk_bp_bp_lists_internal(h->bp, h->d_filt[b], h->batch, h->d_mats, h->mats.data(), s_slot.data(),
+                                    s_view.data(), (int)s_slot.size(), q_slot.data(), q_view.data(),
+                                    (int)q_view.size(), h->compute, band);
 }
 
 // The filling batch is full and more views arrive: backproject the held batch (its launch
 // queues behind the filters already issued, and the next filters write its buffer after it),
 // hold the full one, fill the other buffer.
 int rotate_full(fdk_recon *h) {
-    if (h->held) FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, -1));
+    if (h->held) FDK_TRY(launch_batch(h, h->cur ^ 1, h->batch, -1));
     h->held = true;
-    h->held_first = h->pend_first;
     h->cur ^= 1;
     h->pending = 0;
+    h->bviews[h->cur].clear();
     return FDK_OK;
 }
 
@@ -159,34 +206,39 @@ int flush_all(fdk_recon *h) {
     if (h->held && h->pending > 0) {
         const int nb = fdk_bp_band_count_internal(h->bp);
         for (int b = 0; b < nb; b++) {
-            FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, b));
-            FDK_TRY(launch_batch(h, h->cur, h->pend_first, h->pending, b));
+            FDK_TRY(launch_batch(h, h->cur ^ 1, h->batch, b));
+            FDK_TRY(launch_batch(h, h->cur, h->pending, b));
         }
     } else if (h->held) {
-        FDK_TRY(launch_batch(h, h->cur ^ 1, h->held_first, h->batch, -1));
+        FDK_TRY(launch_batch(h, h->cur ^ 1, h->batch, -1));
     } else if (h->pending > 0) {
-        FDK_TRY(launch_batch(h, h->cur, h->pend_first, h->pending, -1));
+        FDK_TRY(launch_batch(h, h->cur, h->pending, -1));
     }
     h->held = false;
     h->pending = 0;
+    h->bviews[0].clear();
+    h->bviews[1].clear();
     return FDK_OK;
 }
 
 // Filter n raw views (device) into the filling batch behind the views already there; a full
-// batch is held until the next one starts (rotate_full).  Views join a batch only when they
-// continue the waiting views (first == the next view expected); otherwise everything waiting
-// is backprojected first.
+// batch is held until the next one starts (rotate_full).  FP32_EXACT: views join a batch only
+// when they continue the waiting views (first == the next view expected); otherwise everything
+// waiting is backprojected first.  Staged precisions: any views join.
 int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cudaEvent_t release) {
     const fdk_geometry &g = h->g;
     const long long frame = g.nu * g.nv;
     const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
     const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
-    const long long expected = h->pending > 0 ? h->pend_first + h->pending : h->held_first + h->batch;
-    if ((h->pending > 0 || h->held) && first != expected) FDK_TRY(flush_all(h));
+    if (h->precision == FDK_BP_FP32_EXACT && (h->pending > 0 || h->held)) {
+        const long long expected = h->pending > 0 ? (long long)h->bviews[h->cur].back() + 1
+                                                  : (long long)h->bviews[h->cur ^ 1].back() + 1;
+        if (first != expected) FDK_TRY(flush_all(h));
+    }
     for (int done = 0; done < n;) {
         if (h->pending == h->batch) FDK_TRY(rotate_full(h));
-        if (h->pending == 0) h->pend_first = first + done;
         const int m = std::min(n - done, h->batch - h->pending);
+        for (int i = 0; i < m; i++) h->bviews[h->cur].push_back((int)(first + done + i));
         void *dst = static_cast<unsigned char *>(h->d_filt[h->cur]) + (size_t)h->pending * dstride * esz;
         std::pair<cudaEvent_t, cudaEvent_t> t;  // filter time only (the flush below is the BP's)
         FDK_CUDA(cudaEventCreate(&t.first));
@@ -329,6 +381,8 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         s = fdk_bp_create(&h->bp, (int)g->nv, (int)g->nu, 1, (int)g->nx, (int)g->ny, (int)g->nz, &top, &bot,
                           precision, device);
         if (s == FDK_OK && h->d_scale) s = fdk_bp_set_acc_scale_internal(h->bp, h->d_scale);
+        // the quarter-turn kernel where the scan and the grid have the symmetry
+        if (s == FDK_OK) s = fdk_bp_sym_setup_internal(h->bp, h->mats.data(), (int)g->n_proj, &h->sym_rot);
     }
     if (s == FDK_OK) s = wait_stream(h->compute, h->sync_ev[0], "fdk_recon_create");  // set-up copies landed
     if (s != FDK_OK) {
@@ -447,6 +501,12 @@ int fdk_recon_filter_kind(fdk_recon *h, int32_t *kind) {
     return FDK_OK;
 }
 
+int fdk_recon_bp_kernel(fdk_recon *h, int32_t *kind) {
+    FDK_CHECK_ARG(h && kind, "NULL argument");
+    *kind = h->precision == FDK_BP_FP32_EXACT ? 0 : (h->sym_rot ? 2 : 1);
+    return FDK_OK;
+}
+
 int fdk_recon_flush(fdk_recon *h) {
     FDK_ABI_BEGIN
     FDK_CHECK_ARG(h != nullptr, "NULL handle");
@@ -544,6 +604,8 @@ int fdk_recon_reset(fdk_recon *h) {
     h->filter_launches = 0;
     h->pending = 0;  // filtered views not yet backprojected are dropped with the volume
     h->held = false;
+    h->bviews[0].clear();
+    h->bviews[1].clear();
     h->cur = 0;
     return fdk_bp_reset(h->bp);
     FDK_ABI_END

@@ -11,6 +11,7 @@ namespace fdk {
 constexpr long long kWaitLimit = 1ll << 26;
 constexpr unsigned long long kWaitNs = 10ull * 1000 * 1000 * 1000;  // 10 s
 constexpr unsigned kErrTimeout = 1u;
+constexpr unsigned kErrFootprint = 2u;  // a tile's footprint did not fit its shared-memory box
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 

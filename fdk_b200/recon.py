@@ -51,6 +51,14 @@ class Reconstructor:
         check(lib().fdk_recon_filter_kind(self._h, C.byref(k)))
         return "tensor" if k.value == 1 else "fft"
 
+    @property
+    def bp_kernel(self) -> str:
+        """'exact', 'staged' or 'quarter-turn' (the staged kernel plus the quarter-turn kernel for
+        views whose three quarter-turn partners share their batch)."""
+        k = C.c_int32()
+        check(lib().fdk_recon_bp_kernel(self._h, C.byref(k)))
+        return ("exact", "staged", "quarter-turn")[k.value]
+
     def flush(self) -> None:
         """Backproject every filtered view still waiting (a held full batch and the filling one)
         now (asynchronous)."""

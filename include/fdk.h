@@ -267,6 +267,8 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
 /* The reconstructor's compute stream (cudaStream_t as void*), for event timing by the caller. */
 int fdk_recon_stream(fdk_recon *h, void **stream);
 /* Push n raw views (host, nv x nu each, index first..first+n-1; pinned memory overlaps best).
+ * Views may come in any order; a batch of the staged precisions holds whatever views arrived
+ * (FP32_EXACT batches hold consecutive views).
  * The copy to the device runs on a side stream; filtering and backprojection follow on the
  * compute stream.  Returns once the host buffer may be reused. */
 int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t n);
@@ -288,6 +290,12 @@ int fdk_recon_flush(fdk_recon *h);
  * tensor-core GEMM (fdk_toeplitz_*, MIXED precision when nu % 256 == 0 and nv % 128 == 0 on an
  * sm_100 GPU, unless the environment sets FDK_FILTER=fft). */
 int fdk_recon_filter_kind(fdk_recon *h, int32_t *kind);
+/* The backprojection this reconstructor runs: 0 the reference arithmetic (FP32_EXACT), 1 the
+ * staged kernel, 2 the staged kernel plus the quarter-turn kernel: views whose partners
+ * v + N/4, v + N/2, v + 3N/4 (mod N) are in the same batch are backprojected four at a time
+ * with one address computation (a circular scan of N % 4 == 0 views about a square, centred
+ * grid; off when the environment sets FDK_BP_SYM=0).  No counterpart in the reference. */
+int fdk_recon_bp_kernel(fdk_recon *h, int32_t *kind);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);
 /* Volume [z][y][x], x fastest, nz*ny*nx floats (host; the slab pair for a slab reconstructor).

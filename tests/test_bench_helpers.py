@@ -11,11 +11,26 @@ def test_batches_of_in_order_pushes():
     assert bench.count_bp_batches([32 * i for i in range(5, 25)], 32, 512) == [512, 128]
 
 
-def test_batches_break_on_discontinuity():
-    # the views restart (the workload wraps around): the waiting batch is backprojected first
-    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128) == [64, 64]
+def test_batches_break_on_discontinuity_only_for_contiguous_batches():
+    # FP32_EXACT batches hold consecutive views: a restart closes the waiting batch
+    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128, contiguous=True) == [64, 64]
+    # the staged precisions take views in any order
+    assert bench.count_bp_batches([0, 32, 0, 32], 32, 128) == [128]
     # a push larger than a batch fills several batches
     assert bench.count_bp_batches([0], 300, 128) == [128, 128, 44]
+
+
+def test_step_chunks_read_every_view_once_in_quarter_order():
+    import fdk_b200 as F
+
+    p = F.config("c3")
+    seen = sorted(v for b in range(128) for f, n in bench.step_chunks(p, b) for v in range(f, f + n))
+    assert seen == list(range(4096))
+    # each step: 8 views from each quarter, partners v + k N/4 in the same step
+    ch = bench.step_chunks(p, 3)
+    assert [n for _, n in ch] == [8] * 4 and [f - ch[0][0] for f, _ in ch] == [0, 1024, 2048, 3072]
+    # a scan whose quarter does not split into 8-view chunks reads 32 consecutive views
+    assert bench.step_chunks(F.config("c5"), 2) == [(64, 32)]
 
 
 class _Done:

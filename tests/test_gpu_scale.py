@@ -47,9 +47,17 @@ def _views(p, seed, n_ell):
 
 
 def _recon(p, precision, dev, slab=None, batch=None):
+    """Reconstructor fed from device views; the staged precisions read 8 consecutive views from
+    each quarter of the scan in turn, so batches pair views with their quarter-turn partners."""
     r = F.Reconstructor(p, precision, batch=batch or (32 if precision == "fp32_exact" else 256), slab=slab)
-    for c in range(0, p.nProj, 32):
-        r.push_device(dev[c:].data_ptr(), c, min(32, p.nProj - c))
+    if precision == "fp32_exact" or p.nProj % 32:
+        for c in range(0, p.nProj, 32):
+            r.push_device(dev[c:].data_ptr(), c, min(32, p.nProj - c))
+    else:
+        q = p.nProj // 4
+        for b in range(0, q, 8):
+            for k in range(4):
+                r.push_device(dev[b + k * q:].data_ptr(), b + k * q, 8)
     return r
 
 
