@@ -891,8 +891,8 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
 
 // One batch of views held in a device views buffer (n_slots views, any order), for the
 // reconstructor (recon.cu): `n_single` views by (slot, view) through the staged kernel and
-// `n_quad` quarter-turn quadruples (4 slots each, members p, p + N/4, p + N/2, p + 3N/4, and the
-// base view p) through the quarter-turn kernel.  d_mats / host_mats: every view's matrix.
+// `n_quad` quarter-turn quadruples (4 slots each, members b, b + N/4, b + N/2, b + 3N/4 mod N, and
+// the base view b; one per view of each whole orbit) through the quarter-turn kernel.  d_mats / host_mats: every view's matrix.
 // band: -1 = every z band, else one.  Internal to the library.
 int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const float *d_mats, const float *host_mats,
                              const int *s_slot, const int *s_view, int n_single, const int *q_slot,
@@ -954,7 +954,7 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
     }
     FDK_CUDA(cudaEventRecord(tm.second, st));
     h->timers.push_back(tm);
-    if (kb == 0) h->bp_count += n_single + 4ll * n_quad;
+    if (kb == 0) h->bp_count += n_single + n_quad;  // one quadruple per view of a whole orbit
     return FDK_OK;
     FDK_ABI_END
 }

@@ -2,12 +2,14 @@
 // symmetry, for sm_100a.
 //
 // For a circular orbit of N views (N % 4 == 0) about the axis of a square, centred voxel grid,
-// view p + jN/4 sees column T^j(x, y) exactly where view p sees column (x, y): T is a quarter
+// view b + jN/4 sees column T^j(x, y) exactly where view b sees column (x, y): T is a quarter
 // turn of the grid, T(x, y) = (y, n-1-x) or (n-1-y, x) according to the orbit's direction (the
 // host checks which one the matrices follow, and that they do).  So one detector position, one
-// set of bilinear weights and one shared-memory address serve four views, and through the
-// MIRROR element pairs (rows v and nv-1-v) also the mirror voxel nz-1-z of each column: eight
-// voxel updates per index computation instead of two.  This is the reference's own mirror
+// set of bilinear weights and one shared-memory address -- those of base view b at base column
+// c -- serve four (column, view) pairs, (T^j(c), b + jN/4), and through the MIRROR element pairs
+// (rows v and nv-1-v) also the mirror voxel nz-1-z of each: eight voxel updates per index
+// computation instead of two.  With every view of an orbit once as the base, every view reaches
+// every column of the grid.  This is the reference's own mirror
 // shortcut (backprojectionFDK.cu:90-126) extended by the orbit's in-plane symmetry.
 //
 //  * Persistent CTAs walk tiles of one quadrant of the grid (16 x 16 base columns x R top-slab
@@ -85,11 +87,13 @@ struct SymCfg<float2> {
     static constexpr int S = FDK_SYM_FP32_S;
 };
 
-constexpr int kSymMaxQuads = 128;
+constexpr int kSymMaxQuads = 512;
 
-// Quadruples of one launch (kernel parameter): the slots (views-buffer index, the TMA z
-// coordinate) of the four members p, p + N/4, p + N/2, p + 3N/4, and the base view p whose
-// matrix the four share.
+// Quadruples of one launch (kernel parameter, 10 KB): the slots (views-buffer index, the TMA z
+// coordinate) of the four members b, b + N/4, b + N/2, b + 3N/4 (mod N), and the base view b
+// whose matrix the four share.  A batch with whole orbits lists each view once as the base, so
+// every view reaches every column: base columns c through itself, T^j(c) through the quadruple
+// based j quarters earlier.
 struct SymQuads {
     int4 slot[kSymMaxQuads];
     int view[kSymMaxQuads];

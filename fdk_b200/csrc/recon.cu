@@ -143,7 +143,8 @@ int collect_filter_timers(fdk_recon *h) {
 // Backproject the n filtered views of buffer b: every z band (band -1) or one, on the compute
 // stream.  FP32_EXACT: one consecutive run.  Staged precisions: the views whose quarter-turn
 // partners (v mod N/4 equal, one from each quarter of the scan) are in the same batch go to the
-// quarter-turn kernel four at a time, the rest to the staged kernel by (slot, view).
+// quarter-turn kernel -- each such view as the base of one quadruple, its partners as the other
+// three members -- the rest to the staged kernel by (slot, view).
 int launch_batch(fdk_recon *h, int b, int n, int band) {
     const std::vector<int> &vw = h->bviews[b];
     if (h->precision == FDK_BP_FP32_EXACT) {
@@ -164,10 +165,13 @@ int launch_batch(fdk_recon *h, int b, int n, int band) {
             std::vector<int> by_q[4];
             for (size_t k = i; k < j; k++) by_q[e[k][1]].push_back(e[k][2]);
             const size_t nq = std::min({by_q[0].size(), by_q[1].size(), by_q[2].size(), by_q[3].size()});
-            for (size_t k = 0; k < nq; k++) {
-                for (int t = 0; t < 4; t++) q_slot.push_back(by_q[t][k]);
-                q_view.push_back(e[i][0]);
-            }
+            for (size_t k = 0; k < nq; k++)
+                // every member is the base view once: base p + mq with members p + (m + t)q, so
+                // each view reaches every column (base columns c and their turns T^t(c))
+                for (int m = 0; m < 4; m++) {
+                    for (int t = 0; t < 4; t++) q_slot.push_back(by_q[(m + t) & 3][k]);
+                    q_view.push_back(e[i][0] + m * q);
+                }
             for (int t = 0; t < 4; t++)
                 for (size_t k = nq; k < by_q[t].size(); k++) {
                     s_slot.push_back(by_q[t][k]);
