@@ -292,7 +292,9 @@ def test_rtk_staged_kernel_matches_l1_and_oracle(case, monkeypatch):
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
 def test_largest_batches_match_small_ones(precision):
     """Batches of the largest size (512 views; two are held on the device) give the volume of
-    16-view batches up to FP32 summation order, over a scan longer than one batch."""
+    16-view batches up to FP32 summation order, over a scan longer than one batch.  (MIXED: the
+    512-view batch holds 62 whole quarter-turn orbits of the 600-view scan, which the quarter-turn
+    kernel interpolates with its own FP16 arithmetic, so the two differ at the FP16 level.)"""
     import torch
 
     n, views = 32, 600
@@ -309,4 +311,4 @@ def test_largest_batches_match_small_ones(precision):
         vols.append(r.volume())
         assert r.stats()["views"] == views
         r.close()
-    assert rel_l2(vols[0], vols[1]) <= 1e-5
+    assert rel_l2(vols[0], vols[1]) <= (1e-5 if precision == "fp32" else 3e-4)
