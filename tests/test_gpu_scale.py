@@ -171,10 +171,14 @@ def test_c2_slab_pair_mixed_vs_fp64_and_fp32_vs_reference_arithmetic():
     for c in range(0, p.nProj, 64):
         S.add(host[c:c + 64], c)
     got = {k: v[pick].reshape(-1) for k, v in vols.items()}
+    edge = S.edge.astype(bool)
     e_mixed = rel_l2(got["mixed"], S.values)
-    e_fp32 = rel_l2(vols["fp32"], vols["fp32_exact"])
-    print("slab pair: mixed vs fp64", e_mixed, "fp32 vs fp32_exact", e_fp32, "fp32 vs fp64",
-          rel_l2(got["fp32"], S.values), "knife-edge voxels", int(S.edge.sum()))
+    # FP32 (staged) against the reference arithmetic, without the knife-edge voxels of the sampled
+    # slices (columns whose projection touches a detector border in some view); unmasked reported
+    e_fp32 = rel_l2(got["fp32"][~edge], got["fp32_exact"][~edge])
+    print("slab pair: mixed vs fp64", e_mixed, "fp32 vs fp32_exact", e_fp32, "unmasked whole slab",
+          rel_l2(vols["fp32"], vols["fp32_exact"]), "fp32 vs fp64", rel_l2(got["fp32"], S.values),
+          "knife-edge voxels", int(edge.sum()))
     assert e_mixed <= 1e-3 and e_fp32 <= 1e-5
 
 
