@@ -115,6 +115,7 @@ struct BpSymArgs {
     int tiles_z, tz0;    // z tiles of this launch
     int rot;             // quarter turn: > 0 T(x, y) = (y, n-1-x), < 0 T(x, y) = (n-1-y, x)
     unsigned long long wait_ns;
+    int withhold;        // test switch (FDK_BP_TEST_WITHHOLD): CTA 0 never fills its first stage
 };
 
 // Volume offset ([x][y][zs]) of column T^j(x, y), T the launch's quarter turn.
@@ -340,6 +341,7 @@ __global__ void __maxnreg__(FDK_SYM_MAXNREG)
                     ok = false;
                     break;
                 }
+                if (a.withhold && blockIdx.x == 0 && it == 0) continue;  // the consumers' wait runs out
                 const int qd = c * NQ + lane;
                 if (lane < NQ) {
                     TmaMeta &md = meta[s * NQ + lane];
@@ -519,6 +521,7 @@ inline int bp_sym_launch(const BpFastPlan &p, int ctas, float *vol, float *comp,
     a.tiles_z = tze - tzb;
     a.rot = rot;
     a.wait_ns = bp_wait_ns();
+    a.withhold = bp_test_withhold();
     const long long n_tiles = (long long)a.tiles_q * a.tiles_q * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, ctas);

@@ -206,15 +206,22 @@ def test_divvolume_slab_ranks_assemble_the_single_gpu_volume(precision):
             assert rel_l2(got, want) <= (1e-6 if precision == "fp32" else 1e-4), (rank, rel_l2(got, want))
 
 
+@pytest.mark.parametrize("pair", [False, True])
 @pytest.mark.parametrize("precision", ["fp32", "mixed"])
-def test_device_wait_timeout_reports_and_recovers(precision, monkeypatch):
+def test_device_wait_timeout_reports_and_recovers(precision, pair, monkeypatch):
     """FDK_BP_TEST_WITHHOLD makes CTA 0's producer skip its first pipeline stage; with a 1 ms
     wait limit its consumers give up, set the device error word and return, the producer drains
     its own copies (bounded) -- the host sees FDK_ERR_DEVICE_CHECK at the sync.  After a reset
-    (and without the switch) the handle reconstructs as before."""
+    (and without the switch) the handle reconstructs as before.  Both staged kernels: the
+    16 views form 4 whole quarter-turn orbits (pair) or the pairing is off (FDK_BP_SYM=0)."""
     p = small_param(64, 64, 64, 16)
     dev = _views(p, 8, 8)
-    r = _recon(p, precision, dev, batch=16)
+    if not pair:
+        monkeypatch.setenv("FDK_BP_SYM", "0")
+    r = F.Reconstructor(p, precision, batch=16)
+    monkeypatch.delenv("FDK_BP_SYM", raising=False)
+    assert r.bp_kernel == ("quarter-turn" if pair else "staged")
+    r.push_device(dev.data_ptr(), 0, 16)
     want = r.volume().copy()
     r.reset()
     monkeypatch.setenv("FDK_BP_WAIT_NS", "1000000")
