@@ -388,7 +388,7 @@ def reference_gpu_leg(F, param, views, chunks_of, local: int, log) -> dict | Non
     """The reference's own cudaFdkBP (oracle/_ref/libref_gpu_bp.so, compiled for sm_100a) on the
     per-GPU ABCI shape: a 2048 x 2048 x (2 x 256) slab pair (its 32-bit voxel offsets stay valid)
     from 2048^2 views, 32 views per BP() call, next to our precisions on 128 views of the run
-    (in 128-view batches; MIXED also without the quarter-turn pairing)."""
+    (in 128-view batches; FP32 and MIXED also with the other kernel choice, FDK_BP_SYM)."""
     from oracle import oracle as O
 
     import torch
@@ -416,9 +416,10 @@ def reference_gpu_leg(F, param, views, chunks_of, local: int, log) -> dict | Non
            "reference_note": "BP() call = H2D copy of the views + kernel + cudaDeviceSynchronize (stock path)"}
     ours = {}
     pushes = [c for b in range(4) for c in chunks_of(b)]  # 128 views
-    for prec, pair in (("fp32_exact", False), ("fp32", True), ("mixed", True), ("mixed", False)):
-        if not pair:
-            os.environ["FDK_BP_SYM"] = "0"
+    # each precision with the reconstructor's default kernel choice, then the other choice
+    for prec, sym in (("fp32_exact", None), ("fp32", None), ("mixed", None), ("fp32", "0"), ("mixed", "1")):
+        if sym is not None:
+            os.environ["FDK_BP_SYM"] = sym
         r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else 128, device=local, slab=(zc, dc))
         os.environ.pop("FDK_BP_SYM", None)
         for ptr, first, k in pushes[:4]:  # warm-up
@@ -429,7 +430,7 @@ def reference_gpu_leg(F, param, views, chunks_of, local: int, log) -> dict | Non
             r.push_device(ptr, first, k)
         r.sync()
         st = r.stats()
-        key = prec if pair or prec == "fp32_exact" else prec + "_unpaired"
+        key = prec if sym is None else f"{prec}_{r.bp_kernel}"
         ours[key] = {"gups": param.nx * param.ny * 2 * dc * 128 / (st["bp_ms"] * 1e-3) / 1e9, "kernel": r.bp_kernel}
         r.close()
     out["ours"] = ours
@@ -727,8 +728,10 @@ def timed(run, reps: int) -> float:
 
 def kernel_bp(args) -> None:
     """Backprojection batches through the reconstructor on device-resident views (default: the
-    512^3 / 512^2 geometry, 3 batches of 128 views -- views and volume larger than L2, a few GB
-    on the device, small enough for `ncu --set full -k regex:bp_ -s 1 -c 1`)."""
+    512^3 / 512^2 geometry, 3 batches of 128 views read in the bench's quarter order -- views and
+    volume larger than L2, a few GB on the device, small enough for
+    `ncu --set full -k regex:bp_ -s 1 -c 1`).  --variants staged: without the quarter-turn
+    pairing (FDK_BP_SYM=0); --variants paired: with it for MIXED too (FDK_BP_SYM=1)."""
     import torch
 
     import fdk_b200 as F
@@ -737,16 +740,27 @@ def kernel_bp(args) -> None:
     nb, B = args.batches, args.bp_batch
     p = F.config(args.config)
     p.nProj = max(p.nProj, B * nb)  # views over the full circle; more when the run asks for more
+    steps = B * nb // PUSH
+    pushes = [c for b in range(steps) for c in step_chunks(p, b)]
     views = torch.empty((B * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
-    P.project(p, P.phantom_for(p, 2, 20), 0, B * nb, views.data_ptr())
+    ell = P.phantom_for(p, 2, 20)
+    o = 0
+    for first, n in pushes:
+        P.project(p, ell, first, n, views[o:].data_ptr())
+        o += n
+    if args.variants in ("staged", "paired"):
+        os.environ["FDK_BP_SYM"] = "0" if args.variants == "staged" else "1"
     r = F.Reconstructor(p, args.precision, batch=B)
-    for b in range(nb):
-        r.push_device(views[B * b:].data_ptr(), B * b, B)
+    os.environ.pop("FDK_BP_SYM", None)
+    o = 0
+    for first, n in pushes:
+        r.push_device(views[o:].data_ptr(), first, n)
+        o += n
     r.sync()
     st = r.stats()
     st["gups"] = p.nx * p.ny * p.nz * B * nb / (st["bp_ms"] * 1e-3) / 1e9
     print(json.dumps({"kernel": "bp", "config": args.config, "precision": args.precision, "batch": B,
-                      "batches": nb, **st}), flush=True)
+                      "batches": nb, "bp_kernel": r.bp_kernel, **st}), flush=True)
     r.close()
 
 

@@ -563,8 +563,18 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         h->n_bands = nb;
         for (int k = 0; k <= nb; k++) {
             h->band_z[k] = std::min<long long>((long long)k * units / nb * unit, (long long)t.depth);
+            if (k > 0 && k < nb)  // nearest whole unit to an even split of the slices
+                h->band_z[k] = std::min<long long>(((long long)k * t.depth / nb + unit / 2) / unit * unit, t.depth);
             h->band_tz[k] = k == nb ? tiles_z : (int)(h->band_z[k] / R);
         }
+        for (int k = 1; k <= nb; k++)  // rounding must leave no band empty
+            if (h->band_z[k] <= h->band_z[k - 1]) {
+                for (int j = 0; j <= nb; j++) {
+                    h->band_z[j] = std::min<long long>((long long)j * units / nb * unit, (long long)t.depth);
+                    h->band_tz[j] = j == nb ? tiles_z : (int)(h->band_z[j] / R);
+                }
+                break;
+            }
     }
     for (int k = 0; k < kMaxBands && s == FDK_OK; k++)
         ck(cudaEventCreateWithFlags(&h->band_done[k], cudaEventDisableTiming), "event");
@@ -854,14 +864,18 @@ int fdk_bp_band_count_internal(const fdk_bp *h) { return h ? h->n_bands : 1; }
 // Quarter-turn kernel set-up for device-resident batches (recon.cu): returns in *rot the column
 // map of the scan's quarter-turn symmetry, or 0 where the kernel does not apply (FP32_EXACT, not
 // the whole square grid, n_proj % 4 != 0, matrices without the symmetry, a footprint larger
-// than the box, or FDK_BP_SYM=0).  mats: all n_proj views' matrices (host).  Internal.
+// than the box), or is not chosen (MIXED unless FDK_BP_SYM=1; FDK_BP_SYM=0 for every
+// precision).  mats: all n_proj views' matrices (host).  Internal.
 int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot) {
     FDK_CHECK_ARG(h && mats && rot, "NULL argument");
     *rot = 0;
     h->sym_rot = 0;
+    // FDK_BP_SYM: unset = FP32 only (where it measured faster), 1 = FP32 and MIXED, 0 = off
     const char *env = getenv("FDK_BP_SYM");
-    if (env && std::string(env) == "0") return FDK_OK;
+    const std::string mode = env ? env : "";
+    if (mode == "0") return FDK_OK;
     if (h->precision == FDK_BP_FP32_EXACT || !h->plan.tma_ok || !h->sym) return FDK_OK;
+    if (h->precision == FDK_BP_MIXED && mode != "1") return FDK_OK;
     const BpFastPlan &p = h->plan;
     if (p.x0 != 0 || p.y0 != 0 || p.nxs != p.nys || p.nxs != h->nx || h->nx != h->ny || (p.nxs & 1) || n_proj % 4)
         return FDK_OK;

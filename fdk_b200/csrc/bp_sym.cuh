@@ -44,45 +44,69 @@
 namespace fdk {
 
 #ifndef FDK_SYM_MIXED_R
-#define FDK_SYM_MIXED_R 8
+#define FDK_SYM_MIXED_R 6
 #endif
 #ifndef FDK_SYM_MIXED_BW
-#define FDK_SYM_MIXED_BW 24
+#define FDK_SYM_MIXED_BW 20
 #endif
 #ifndef FDK_SYM_MIXED_NQ
-#define FDK_SYM_MIXED_NQ 2
+#define FDK_SYM_MIXED_NQ 4
 #endif
 #ifndef FDK_SYM_MIXED_S
 #define FDK_SYM_MIXED_S 2
 #endif
+#ifndef FDK_SYM_MIXED_BH
+#define FDK_SYM_MIXED_BH 32
+#endif
 #ifndef FDK_SYM_FP32_R
-#define FDK_SYM_FP32_R 8
+#define FDK_SYM_FP32_R 6
+#endif
+#ifndef FDK_SYM_FP32_BW
+#define FDK_SYM_FP32_BW 18
+#endif
+#ifndef FDK_SYM_FP32_BH
+#define FDK_SYM_FP32_BH 32
 #endif
 #ifndef FDK_SYM_FP32_NQ
-#define FDK_SYM_FP32_NQ 1
+#define FDK_SYM_FP32_NQ 2
 #endif
 #ifndef FDK_SYM_FP32_S
-#define FDK_SYM_FP32_S 2
+#define FDK_SYM_FP32_S 3
 #endif
 #ifndef FDK_SYM_INTERP
 #define FDK_SYM_INTERP 0
 #endif
 
+// Tile and pipeline shapes (macros for tuning sweeps), measured on one B200 (GUPS of the kernel,
+// 512-view batches in the bench's quarter read order; staged = bp_tma_kernel on the same views):
+//   FP32:  C2 1227 staged -> 1777 (R 6, 34 x 40 boxes, 1 quad x 2 stages) -> 1908 (18 x 32 boxes,
+//          2 quads x 3 stages); C3 1257 staged -> 1749.  R 4 at 64 registers (3 CTAs per SM):
+//          1895 at C2 but 1426 at C3 (short volume runs).
+//   MIXED: C2 2320 staged against 2090-2229 for every shape tried (R 4-6, 20-28 x 32-40 boxes,
+//          2-4 quads, 2-4 stages, 2 or 3 CTAs per SM, FP16 or mixed-FMA interpolation); C3 2358
+//          staged against 2084.  The FP16 kernel sits near 57% of its shared-memory wavefront
+//          bound (issue 39%, latency-bound at 4 consumer warps per scheduler and 96 registers)
+//          while the FP32 one saturates its bound; the reconstructor therefore pairs views for
+//          FP32 only unless FDK_BP_SYM=1.
+// At 112 registers (one CTA per SM: 9 warps) both ran at 1440-1630.
 template <typename E>
 struct SymCfg;
 template <>
 struct SymCfg<__half2> {
-    static constexpr int R = FDK_SYM_MIXED_R;    // top-slab slices per thread
-    static constexpr int BW = FDK_SYM_MIXED_BW;  // box width (v elements; x 4 B a multiple of 16 B)
-    static constexpr int BH = 40;                // box height (u rows)
+    static constexpr int R = FDK_SYM_MIXED_R;    // top-slab slices per thread (registers: see below)
+    // box width (v elements; x 4 B a multiple of 16 B).  The row pitch sets the bank pattern of
+    // the 8 x 4 lane block, whose samples fall on about ten rows at nearly the same v: 20 or 28
+    // words repeat every 8 rows, 24 words every 4 (2-3x the shared wavefronts).
+    static constexpr int BW = FDK_SYM_MIXED_BW;
+    static constexpr int BH = FDK_SYM_MIXED_BH;  // box height (u rows)
     static constexpr int NQ = FDK_SYM_MIXED_NQ;  // quadruples per stage
     static constexpr int S = FDK_SYM_MIXED_S;    // stages
 };
 template <>
 struct SymCfg<float2> {
     static constexpr int R = FDK_SYM_FP32_R;
-    static constexpr int BW = 24;
-    static constexpr int BH = 40;
+    static constexpr int BW = FDK_SYM_FP32_BW;  // 2 BW words a row; = 4 mod 32 (BW = 2 mod 16): 8-row bank period
+    static constexpr int BH = FDK_SYM_FP32_BH;
     static constexpr int NQ = FDK_SYM_FP32_NQ;
     static constexpr int S = FDK_SYM_FP32_S;
 };
@@ -194,6 +218,8 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
     constexpr int R = C::R;
     constexpr unsigned BOX = sym_box_bytes<E>();
     const float *m = md.m;
+    const bool interior = md.interior;  // read once: md lives in shared memory
+    const int u_lo = md.u_lo, v_lo = md.v_lo;
     const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
     const float rw = __fdividef(1.0f, w);
     const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
@@ -210,13 +236,13 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
         const __half2 one = __float2half2_rn(1.f);
         {  // staged: the host checked that every tile's footprint fits the box (sym_footprints_fit)
-            const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
+            const float C0 = fmaf(A - (float)v_lo, 1024.f, 12582912.f);
             const float B1 = B * 1024.f;
-            const unsigned rowp = box + (unsigned)(u0 - md.u_lo) * RB - (0x4B400000u >> 10) * 4u;
+            const unsigned rowp = box + (unsigned)(u0 - u_lo) * RB - (0x4B400000u >> 10) * 4u;
 #pragma unroll
             for (int k = 0; k < R; k++) {
                 bool mv = true, rv = true;
-                if (!md.interior) {
+                if (!interior) {
                     // slices near the detector's top or bottom edge: SUBPIXEL's bounds per slice
                     const float v = fmaf(B, (float)k, A);
                     const float vr = (float)(nv - 1) - v;
@@ -237,7 +263,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
                     const __half2 e0 = u2h(lds32(a + j * BOX)), e1 = u2h(lds32(a + j * BOX + 4));
                     const __half2 e2 = u2h(lds32(a + j * BOX + RB)), e3 = u2h(lds32(a + j * BOX + RB + 4));
 #if FDK_SYM_INTERP == 1
-                    if (md.interior) {
+                    if (interior) {
                         mixed_fma4(am[j][k], ar[j][k], e0, e1, e2, e3, w01, w23);
                     } else {
                         float tm = 0.f, tr = 0.f;
@@ -247,7 +273,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
                     }
 #else
                     const __half2 r = __hfma2(e3, w3, __hfma2(e2, w2, __hfma2(e1, w1, __hmul2(e0, w0))));
-                    if (md.interior) {
+                    if (interior) {
                         acc_add_f16x2(am[j][k], ar[j][k], r);
                     } else {
                         const float2 rf = __half22float2(r);
@@ -267,7 +293,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
             const float v = fmaf(B, (float)k, A);
             bool mv = true, rv = true;
             float vf;
-            if (!md.interior) {
+            if (!interior) {
                 const float vr = (float)(nv - 1) - v;
                 mv = v >= 0.f && v < (float)(nv - 1);
                 rv = vr >= 0.f && vr < (float)(nv - 1);
@@ -280,7 +306,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
             const float fv = v - vf;
             const float w1 = wa * fv, w3 = wb * fv;
             const float w0 = wa - w1, w2 = wb - w3;
-            const unsigned a = box + (unsigned)(((u0 - md.u_lo) * C::BW + (vi - md.v_lo)) * 8);
+            const unsigned a = box + (unsigned)(((u0 - u_lo) * C::BW + (vi - v_lo)) * 8);
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const float2 e0 = lds64f(a + j * BOX), e1 = lds64f(a + j * BOX + 8);
@@ -295,7 +321,10 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
 }
 
 #ifndef FDK_SYM_MAXNREG
-#define FDK_SYM_MAXNREG 112  // 2 CTAs of 288 threads per SM: 2 x 9 warps x 32 x 112 <= 65536
+// 2 CTAs of 288 threads per SM: registers are allocated for an even number of warps (10 of
+// the 9), so 2 x 10 x 32 x 96 <= 65536.  (At 112 the SM held one CTA: 9 warps, 14% active.)
+// With 4 x 2 x R accumulators, R = 6 fits without spills (R = 8 spills at 96).
+#define FDK_SYM_MAXNREG 96
 #endif
 template <typename E>
 __global__ void __maxnreg__(FDK_SYM_MAXNREG)
@@ -337,7 +366,7 @@ __global__ void __maxnreg__(FDK_SYM_MAXNREG)
             for (int c = 0; c < n_chunks; c++, it++) {
                 const int s = it % S;
                 const unsigned ph = (unsigned)(it / S) & 1u;
-                if (it >= S && !mbar_wait(empty0 + 8 * s, ph ^ 1u, a.wait_ns)) {
+                if (it >= S && !mbar_wait_backoff(empty0 + 8 * s, ph ^ 1u, a.wait_ns, FDK_PRODUCER_SLEEP_NS)) {
                     ok = false;
                     break;
                 }
@@ -469,6 +498,8 @@ template <typename E>
 inline int sym_prepare(int &ctas, int device) {
     const int smem = sym_smem_bytes<E>();
     FDK_CUDA(cudaFuncSetAttribute(bp_sym_kernel<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    // room for two CTAs' boxes per SM
+    FDK_CUDA(cudaFuncSetAttribute(bp_sym_kernel<E>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     int per_sm = 0, sms = 0;
     FDK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bp_sym_kernel<E>, 288, smem));
     FDK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));

@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
             for (int c = 0; c < n_chunks; c++, it++) {
                 const int s = it % S;
                 const unsigned ph = (unsigned)(it / S) & 1u;
-                if (it >= S && !mbar_wait(empty0 + 8 * s, ph ^ 1u, a.wait_ns)) {
+                if (it >= S && !mbar_wait_backoff(empty0 + 8 * s, ph ^ 1u, a.wait_ns, FDK_PRODUCER_SLEEP_NS)) {
                     ok = false;
                     break;
                 }

@@ -9,6 +9,10 @@
 namespace fdk {
 
 constexpr long long kWaitLimit = 1ll << 26;
+// Sleep between a producer warp's polls of a stage's empty barrier (tuning macro; 0 = spin).
+#ifndef FDK_PRODUCER_SLEEP_NS
+#define FDK_PRODUCER_SLEEP_NS 0
+#endif
 constexpr unsigned long long kWaitNs = 10ull * 1000 * 1000 * 1000;  // 10 s
 constexpr unsigned kErrTimeout = 1u;
 constexpr unsigned kErrFootprint = 2u;  // a tile's footprint did not fit its shared-memory box
@@ -42,6 +46,29 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigne
             : "memory");
         if (ok) return true;
         if ((i & 255) == 0) {
+            const unsigned long long t = global_ns();
+            if (i == 0) t0 = t;
+            else if (t - t0 > limit_ns) return false;
+        }
+    }
+    return false;
+}
+// The same wait for a warp that usually finds the phase incomplete (a producer waiting for
+// consumers to free a stage): between polls it sleeps sleep_ns, so its polling does not take
+// issue slots from the warps doing the work.
+__device__ __forceinline__ bool mbar_wait_backoff(unsigned bar, unsigned parity, unsigned long long limit_ns,
+                                                  unsigned sleep_ns) {
+    unsigned long long t0 = 0;
+    for (long long i = 0; i < kWaitLimit; i++) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (sleep_ns) __nanosleep(sleep_ns);
+        if ((i & 15) == 0) {
             const unsigned long long t = global_ns();
             if (i == 0) t0 = t;
             else if (t - t0 > limit_ns) return false;

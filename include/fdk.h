@@ -294,7 +294,8 @@ int fdk_recon_filter_kind(fdk_recon *h, int32_t *kind);
  * staged kernel, 2 the staged kernel plus the quarter-turn kernel: views whose partners
  * v + N/4, v + N/2, v + 3N/4 (mod N) are in the same batch are backprojected four at a time
  * with one address computation (a circular scan of N % 4 == 0 views about a square, centred
- * grid; off when the environment sets FDK_BP_SYM=0).  No counterpart in the reference. */
+ * grid).  FP32 uses it by default; MIXED only when the environment sets FDK_BP_SYM=1 (its
+ * staged kernel measured faster); FDK_BP_SYM=0 turns it off.  No counterpart in the reference. */
 int fdk_recon_bp_kernel(fdk_recon *h, int32_t *kind);
 /* Wait (bounded by timeout_ms; <= 0 means 10 minutes) until every pushed view is backprojected. */
 int fdk_recon_sync(fdk_recon *h, int64_t timeout_ms);

@@ -216,8 +216,7 @@ def test_device_wait_timeout_reports_and_recovers(precision, pair, monkeypatch):
     16 views form 4 whole quarter-turn orbits (pair) or the pairing is off (FDK_BP_SYM=0)."""
     p = small_param(64, 64, 64, 16)
     dev = _views(p, 8, 8)
-    if not pair:
-        monkeypatch.setenv("FDK_BP_SYM", "0")
+    monkeypatch.setenv("FDK_BP_SYM", "1" if pair else "0")
     r = F.Reconstructor(p, precision, batch=16)
     monkeypatch.delenv("FDK_BP_SYM", raising=False)
     assert r.bp_kernel == ("quarter-turn" if pair else "staged")

@@ -24,8 +24,7 @@ def quarter_order(n_proj, chunk):
 
 
 def run(p, precision, proj, order, batch, pair=True, slab=None):
-    if not pair:
-        os.environ["FDK_BP_SYM"] = "0"
+    os.environ["FDK_BP_SYM"] = "1" if pair else "0"  # MIXED pairs only on request
     try:
         r = F.Reconstructor(p, precision, batch=batch, slab=slab)
     finally:
@@ -75,6 +74,19 @@ def test_quadruples_and_unpaired_views_in_one_batch(precision):
     assert rel_l2(got[m], ref[m]) <= (3e-6 if precision == "fp32" else 5e-4)
 
 
+def test_default_pairing_is_fp32_only():
+    """Without FDK_BP_SYM the FP32 reconstructor pairs views and the MIXED one runs the staged
+    kernel (measured faster for FP16 views)."""
+    os.environ.pop("FDK_BP_SYM", None)
+    p = small_param(32, 32, 32, 16)
+    kinds = {}
+    for prec in ("fp32", "mixed", "fp32_exact"):
+        r = F.Reconstructor(p, prec, batch=16)
+        kinds[prec] = r.bp_kernel
+        r.close()
+    assert kinds == {"fp32": "quarter-turn", "mixed": "staged", "fp32_exact": "exact"}
+
+
 def test_pairing_switches_off_without_the_symmetry():
     """A grid that is not square, a view count that is not a multiple of 4, and a sub-slab reach
     the staged kernel alone; results still match the oracle."""
@@ -99,8 +111,7 @@ def test_full_size_c2_paired_matches_unpaired():
     torch.cuda.synchronize()
     vols = {}
     for pair in (True, False):
-        if not pair:
-            os.environ["FDK_BP_SYM"] = "0"
+        os.environ["FDK_BP_SYM"] = "1" if pair else "0"
         r = F.Reconstructor(p, "mixed", batch=256)
         os.environ.pop("FDK_BP_SYM", None)
         for first, n in quarter_order(p.nProj, 8):
