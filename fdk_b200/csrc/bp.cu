@@ -420,8 +420,9 @@ bool quarter_turn_holds(const float *mats, int n_proj, int n, int nz, int rot) {
 
 // Every tile of the quadrant (16 x 16 columns x R slices of the top slab [z0, z0 + nzz)) fits
 // the kernel's BW x BH box in every base view.  The map is linear-fractional, so a tile's
-// extremes sit at its corner columns; the box's u extent is at most umax - umin + 5 and its v
-// extent at most (vmax - vmin) + 7 (floors, margins, 16-byte alignment), and vmax - vmin over a
+// extremes sit at its corner columns; the box's u extent (floor(umax) + 2 - (floor(umin) - 1) + 1)
+// is below umax - umin + 5 and its v extent (the same with the start rounded down to 4 elements
+// for the 16-byte rule) below vmax - vmin + 8, and vmax - vmin over a
 // tile (a max minus a min of functions linear in the tile's first slice) is convex along z, so
 // the first and last z tiles bound every z tile.
 bool sym_footprints_fit(const float *mats, int n_proj, int n, int z0, int nzz, int R, int BW, int BH) {
@@ -450,7 +451,7 @@ bool sym_footprints_fit(const float *mats, int n_proj, int n, int z0, int nzz, i
                     }
                 }
                 for (int e = 0; e < 2; e++) spread = std::max(spread, vhi[e] - vlo[e]);
-                if (umax - umin + 5.01 > BH || spread + 7.01 > BW) return false;
+                if (umax - umin + 5.01 > BH || spread + 8.01 > BW) return false;
             }
     }
     return true;
