@@ -419,16 +419,16 @@ bool quarter_turn_holds(const float *mats, int n_proj, int n, int nz, int rot) {
 }
 
 // Every tile of the quadrant (16 x 16 columns x R slices of the top slab [z0, z0 + nzz)) fits
-// the kernel's BW x BH box in every base view.  The map is linear-fractional, so a tile's
+// the kernel's BW x BH box in every view (each view is the base of a quadruple).  The map is linear-fractional, so a tile's
 // extremes sit at its corner columns; the box's u extent (floor(umax) + 2 - (floor(umin) - 1) + 1)
 // is below umax - umin + 5 and its v extent (the same with the start rounded down to 4 elements
 // for the 16-byte rule) below vmax - vmin + 8, and vmax - vmin over a
 // tile (a max minus a min of functions linear in the tile's first slice) is convex along z, so
 // the first and last z tiles bound every z tile.
 bool sym_footprints_fit(const float *mats, int n_proj, int n, int z0, int nzz, int R, int BW, int BH) {
-    const int q = n_proj / 4, half = n / 2, tq = (half + 15) / 16;
+    const int half = n / 2, tq = (half + 15) / 16;
     const int last = z0 + (int)((ceil_div(nzz, R) - 1) * R);
-    for (int p = 0; p < q; p++) {
+    for (int p = 0; p < n_proj; p++) {  // every view is the base of a quadruple
         const float *m = mats + 12 * (long long)p;
         for (int tx = 0; tx < tq; tx++)
             for (int ty = 0; ty < tq; ty++) {
