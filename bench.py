@@ -256,14 +256,18 @@ BATCH = 512  # views per backprojection batch (every 16th step); --bp-batch chan
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
 
 
-def step_chunks(param, b: int, B: int = PUSH) -> list:
-    """The views of step b as (first, count) chunks: B/4 consecutive views from each quarter of
-    the scan (view v + k N/4, k = 0..3), the read order in which every batch holds whole
+READ_ORDER = "quarter"  # set by main(): "quarter" or "sequential"
+
+
+def step_chunks(param, b: int, B: int = PUSH, order: str | None = None) -> list:
+    """The views of step b as (first, count) chunks.  Quarter order: B/4 consecutive views from
+    each quarter of the scan (view v + k N/4, k = 0..3), in which every batch holds whole
     quarter-turn quadruples (fdk_recon_bp_kernel); all 128 steps of the 4096-view scan read each
-    view once.  Scans whose quarter is not a multiple of B/4 views read B consecutive views."""
+    view once.  Sequential order, and scans whose quarter is not a multiple of B/4 views: B
+    consecutive views."""
     N = param.nProj
     c = B // 4
-    if B % 4 == 0 and N % 4 == 0 and (N // 4) % c == 0:
+    if (order or READ_ORDER) == "quarter" and B % 4 == 0 and N % 4 == 0 and (N // 4) % c == 0:
         q = N // 4
         base = (b * c) % q
         return [(base + k * q, c) for k in range(4)]
@@ -331,7 +335,7 @@ def errors(got: np.ndarray, want: np.ndarray, mask=None) -> dict:
 
 
 def accuracy_leg(F, param, views, chunks_of, steps: int, slab, local: int, log) -> dict:
-    """The run's views (steps 0..steps-1, chunks_of(b) -> (device pointer, first view, count)),
+    """The run's views (steps 0..steps-1, chunks_of(b) -> (device pointer, view indices)),
     reconstructed at full size in MIXED and FP32, against the FP64 oracle (checker only) at 1e5
     seeded voxels and every voxel of the central x, y and z slices of this rank's slab pair; then
     FP32 (staged) against the reference kernel's arithmetic (fp32_exact, bit-identical to
@@ -348,22 +352,28 @@ def accuracy_leg(F, param, views, chunks_of, steps: int, slab, local: int, log) 
     inside = ((vox[:, 2] >= z0) & (vox[:, 2] < z0 + d)) | ((vox[:, 2] >= param.nz - z0 - d) &
                                                              (vox[:, 2] < param.nz - z0))
     vox = np.ascontiguousarray(vox[inside])
-    pushes = [c for b in range(steps) for c in chunks_of(b)]
-    got = {}
+    pushes = [chunks_of(b) for b in range(steps)]
+    got, kind = {}, {}
     for prec in ("mixed", "fp32"):
         r = F.Reconstructor(param, prec, batch=BATCH, device=local, slab=slab)
-        for ptr, first, n in pushes:
-            r.push_device(ptr, first, n)
+        for ptr, ids in pushes:
+            r.push_device_views(ptr, ids)
         got[prec] = r.sample(vox)
-        kind = r.bp_kernel
+        kind[prec] = r.bp_kernel
         r.close()
     S = O.SampledFDK(param, vox)
     frame = param.nu * param.nv
-    for ptr, first, n in pushes:
+    for ptr, ids in pushes:
         i = (ptr - views.data_ptr()) // (4 * frame)
-        S.add(views[i:i + n].cpu().numpy(), first)
+        j = 0
+        while j < len(ids):  # the oracle takes runs of consecutive views
+            k = j + 1
+            while k < len(ids) and ids[k] == ids[k - 1] + 1:
+                k += 1
+            S.add(views[i + j:i + k].cpu().numpy(), int(ids[j]))
+            j = k
     mask = S.edge.astype(bool)
-    n_views = sum(n for _, _, n in pushes)
+    n_views = sum(len(ids) for _, ids in pushes)
     res = {"vs": "fp64 oracle (sampled)", "views": n_views, "bp_kernel": kind,
            "voxels": f"{len(vox)}: 1e5 seeded random voxels + the central x, y and z slices (within the slab pair)",
            "mixed": errors(got["mixed"], S.values, mask), "fp32": errors(got["fp32"], S.values, mask)}
@@ -373,8 +383,8 @@ def accuracy_leg(F, param, views, chunks_of, steps: int, slab, local: int, log) 
     vols = {}
     for prec in ("fp32", "fp32_exact"):
         r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else BATCH, device=local, slab=(zc, dc))
-        for ptr, first, n in pushes:
-            r.push_device(ptr, first, n)
+        for ptr, ids in pushes:
+            r.push_device_views(ptr, ids)
         vols[prec] = r.volume().astype(np.float64)
         r.close()
     res["fp32_vs_fp32_exact"] = {"slab_pair": [zc, dc], **errors(vols["fp32"], vols["fp32_exact"])}
@@ -415,19 +425,18 @@ def reference_gpu_leg(F, param, views, chunks_of, local: int, log) -> dict | Non
            "reference_bp_call_gups": upd / (ref["call_ms"] * 1e-3) / 1e9,
            "reference_note": "BP() call = H2D copy of the views + kernel + cudaDeviceSynchronize (stock path)"}
     ours = {}
-    pushes = [c for b in range(4) for c in chunks_of(b)]  # 128 views
+    pushes = [chunks_of(b) for b in range(4)]  # 128 views
     # each precision with the reconstructor's default kernel choice, then the other choice
     for prec, sym in (("fp32_exact", None), ("fp32", None), ("mixed", None), ("fp32", "0"), ("mixed", "1")):
         if sym is not None:
             os.environ["FDK_BP_SYM"] = sym
         r = F.Reconstructor(param, prec, batch=32 if prec == "fp32_exact" else 128, device=local, slab=(zc, dc))
         os.environ.pop("FDK_BP_SYM", None)
-        for ptr, first, k in pushes[:4]:  # warm-up
-            r.push_device(ptr, first, k)
+        r.push_device_views(*pushes[0])  # warm-up
         r.sync()
         r.reset()
-        for ptr, first, k in pushes:
-            r.push_device(ptr, first, k)
+        for ptr, ids in pushes:
+            r.push_device_views(ptr, ids)
         r.sync()
         st = r.stats()
         key = prec if sym is None else f"{prec}_{r.bp_kernel}"
@@ -492,19 +501,14 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     log(f"generated {n_dev_views} views ({n_dev_views * frame * 4 / GIB:.1f} GiB) in HBM")
 
     def chunks_of(b):
-        """Step b's pushes: (device pointer, first view, count)."""
-        o = (b % pool_steps) * B
-        out = []
-        for first, n in step_chunks(param, b):
-            out.append((views[o:].data_ptr(), first, n))
-            o += n
-        return out
+        """Step b's push: (device pointer of its B views in the pool, their view indices)."""
+        ids = np.array([v for first, n in step_chunks(param, b) for v in range(first, first + n)], np.int64)
+        return views[(b % pool_steps) * B:].data_ptr(), ids
 
     def timed_device_run(precision: str, steps: int, warmup: int):
         r = F.Reconstructor(param, precision, batch=BATCH, device=local, slab=slab)
         for b in range(warmup):
-            for ptr, first, n in chunks_of(b):
-                r.push_device(ptr, first, n)
+            r.push_device_views(*chunks_of(b))
         r.sync()
         st0 = r.stats()
         l0 = r.launch_count
@@ -513,8 +517,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for b in range(warmup, warmup + steps):
-            for ptr, first, n in chunks_of(b):
-                r.push_device(ptr, first, n)
+            r.push_device_views(*chunks_of(b))
         r.flush()  # backproject a last partial batch inside the timed region
         e1.record(stream)
         e1.synchronize()
@@ -583,23 +586,20 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         torch.cuda.empty_cache()
         host_steps = pool // B
 
-        def host_chunks(b):
-            o = (b % host_steps) * B
-            for first, n in step_chunks(param, b % pool_steps):
-                yield host_views[o:].data_ptr(), first, n
-                o += n
+        def host_step(b):
+            ids = np.array([v for first, n in step_chunks(param, b % pool_steps) for v in range(first, first + n)],
+                           np.int64)
+            return host_views[(b % host_steps) * B:].data_ptr(), ids
 
         re = F.Reconstructor(param, args.precision, batch=BATCH, device=local, slab=slab)
         for b in range(args.warmup):
-            for ptr, first, n in host_chunks(b):
-                re.push_ptr(ptr, first, n)
+            re.push_views_ptr(*host_step(b))
         re.sync()
         re.reset()
         barrier()
         t0 = time.perf_counter()
         for b in range(args.steps):
-            for ptr, first, n in host_chunks(b):
-                re.push_ptr(ptr, first, n)
+            re.push_views_ptr(*host_step(b))
         if host_vol is not None:
             re.volume_into(host_vol.data_ptr())
         else:
@@ -701,8 +701,10 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": n_launches,
             "filter": filter_kind, "bp_kernel": bp_kind,
-            "read_order": ("each step reads 8 consecutive views from each quarter of the scan (views v + k N/4); "
-                           "the 128 steps read every view once"),
+            "read_order": (READ_ORDER + (": each step reads 8 consecutive views from each quarter of the scan "
+                                         "(views v + k N/4)" if READ_ORDER == "quarter" else
+                                         ": each step reads 32 consecutive views") +
+                           "; the 128 steps of the whole scan read every view once"),
             "plain_fp32": fp32, "accuracy": acc, "reference_gpu": ref_gpu,
         }
         print(json.dumps(out), flush=True)
@@ -741,7 +743,7 @@ def kernel_bp(args) -> None:
     p = F.config(args.config)
     p.nProj = max(p.nProj, B * nb)  # views over the full circle; more when the run asks for more
     steps = B * nb // PUSH
-    pushes = [c for b in range(steps) for c in step_chunks(p, b)]
+    pushes = [c for b in range(steps) for c in step_chunks(p, b, order="quarter")]
     views = torch.empty((B * nb, p.nv, p.nu), dtype=torch.float32, device="cuda")
     ell = P.phantom_for(p, 2, 20)
     o = 0
@@ -870,8 +872,17 @@ def kernel_learned(args) -> None:
                       "ms_per_step": 1e3 * (time.perf_counter() - t0) / args.reps, "mse": e}), flush=True)
 
 
+def pairs_views(param, precision: str) -> bool:
+    """Whether the reconstructor pairs views into quarter-turn quadruples for this precision by
+    default (fdk_recon_bp_kernel): FP32 (MIXED with FDK_BP_SYM=1) on a square grid from a scan of
+    N % 4 == 0 views; the library's own checks decide in the end."""
+    sym = os.environ.get("FDK_BP_SYM", "")
+    on = (precision == "fp32" and sym != "0") or (precision == "mixed" and sym == "1")
+    return on and param.nx == param.ny and param.nProj % 4 == 0
+
+
 def main():
-    global BATCH
+    global BATCH, READ_ORDER
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=128)
@@ -888,6 +899,9 @@ def main():
     ap.add_argument("--batches", type=int, default=3, help="--kernel bp: batches")
     ap.add_argument("--reps", type=int, default=3, help="--kernel filter/rtk/learned: timed repetitions")
     ap.add_argument("--variants", default="", help="--kernel filter/rtk: comma-separated variants")
+    ap.add_argument("--read-order", choices=["auto", "quarter", "sequential"], default="auto",
+                    help="views per step: 8 from each quarter of the scan, or 32 consecutive (auto: quarter "
+                         "where the reconstructor pairs views)")
     args = ap.parse_args()
     if args.kernel:
         defaults = {"bp": ("c2", 128), "filter": ("c4", 128), "rtk": ("c2", 32), "learned": ("c5", 90)}
@@ -901,6 +915,8 @@ def main():
     from fdk_b200.geometry import config
 
     param = config(args.config or "c3")
+    READ_ORDER = args.read_order if args.read_order != "auto" else (
+        "quarter" if pairs_views(param, args.precision) else "sequential")
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))

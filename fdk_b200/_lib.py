@@ -42,6 +42,7 @@ EXPORTED = [
     "fdk_bp_sample", "fdk_bp_stats", "fdk_bp_reset", "fdk_bp_destroy",
     "fdk_rtk_reconstruct_conebeam", "fdk_rtk_backproject_device", "fdk_rtk_sync",
     "fdk_recon_create", "fdk_recon_create_slab", "fdk_recon_stream", "fdk_recon_push", "fdk_recon_push_device",
+    "fdk_recon_push_views", "fdk_recon_push_device_views",
     "fdk_recon_push_folder", "fdk_recon_flush", "fdk_recon_filter_kind", "fdk_recon_bp_kernel", "fdk_recon_sync",
     "fdk_recon_get_volume", "fdk_recon_sample", "fdk_recon_stats", "fdk_recon_launch_count", "fdk_recon_reset", "fdk_recon_destroy",
     "fdk_phantom_project", "fdk_forward_project", "fdk_probe_smem", "fdk_probe_fma",
@@ -138,6 +139,8 @@ def lib() -> C.CDLL:
         "fdk_recon_stream": ([vp, C.POINTER(vp)], C.c_int),
         "fdk_recon_push": ([vp, vp, i64, i64], C.c_int),
         "fdk_recon_push_device": ([vp, vp, i64, i64], C.c_int),
+        "fdk_recon_push_views": ([vp, vp, vp, i64], C.c_int),
+        "fdk_recon_push_device_views": ([vp, vp, vp, i64], C.c_int),
         "fdk_recon_push_folder": ([vp, C.c_char_p, i64, i64, i32, i32, i32], C.c_int),
         "fdk_recon_flush": ([vp], C.c_int),
         "fdk_recon_filter_kind": ([vp, C.POINTER(i32)], C.c_int),

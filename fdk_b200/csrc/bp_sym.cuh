@@ -47,10 +47,10 @@ namespace fdk {
 #define FDK_SYM_MIXED_R 6
 #endif
 #ifndef FDK_SYM_MIXED_BW
-#define FDK_SYM_MIXED_BW 20
+#define FDK_SYM_MIXED_BW 28
 #endif
 #ifndef FDK_SYM_MIXED_NQ
-#define FDK_SYM_MIXED_NQ 4
+#define FDK_SYM_MIXED_NQ 3
 #endif
 #ifndef FDK_SYM_MIXED_S
 #define FDK_SYM_MIXED_S 2
@@ -62,7 +62,7 @@ namespace fdk {
 #define FDK_SYM_FP32_R 6
 #endif
 #ifndef FDK_SYM_FP32_BW
-#define FDK_SYM_FP32_BW 18
+#define FDK_SYM_FP32_BW 26
 #endif
 #ifndef FDK_SYM_FP32_BH
 #define FDK_SYM_FP32_BH 32
@@ -71,7 +71,7 @@ namespace fdk {
 #define FDK_SYM_FP32_NQ 2
 #endif
 #ifndef FDK_SYM_FP32_S
-#define FDK_SYM_FP32_S 3
+#define FDK_SYM_FP32_S 2
 #endif
 #ifndef FDK_SYM_INTERP
 #define FDK_SYM_INTERP 0
@@ -96,7 +96,8 @@ struct SymCfg<__half2> {
     static constexpr int R = FDK_SYM_MIXED_R;    // top-slab slices per thread (registers: see below)
     // box width (v elements; x 4 B a multiple of 16 B).  The row pitch sets the bank pattern of
     // the 8 x 4 lane block, whose samples fall on about ten rows at nearly the same v: 20 or 28
-    // words repeat every 8 rows, 24 words every 4 (2-3x the shared wavefronts).
+    // words repeat every 8 rows, 24 words every 4 (2-3x the shared wavefronts); 28 also leaves
+    // room for the volume's top and bottom tiles (footprint check).
     static constexpr int BW = FDK_SYM_MIXED_BW;
     static constexpr int BH = FDK_SYM_MIXED_BH;  // box height (u rows)
     static constexpr int NQ = FDK_SYM_MIXED_NQ;  // quadruples per stage
@@ -105,7 +106,9 @@ struct SymCfg<__half2> {
 template <>
 struct SymCfg<float2> {
     static constexpr int R = FDK_SYM_FP32_R;
-    static constexpr int BW = FDK_SYM_FP32_BW;  // 2 BW words a row; = 4 mod 32 (BW = 2 mod 16): 8-row bank period
+    // 2 BW words a row: 52 words (= 20 mod 32) repeats every 8 rows, as 36 (= 4); 26 elements
+    // also leave room for the volume's top and bottom tiles (footprint check)
+    static constexpr int BW = FDK_SYM_FP32_BW;
     static constexpr int BH = FDK_SYM_FP32_BH;
     static constexpr int NQ = FDK_SYM_FP32_NQ;
     static constexpr int S = FDK_SYM_FP32_S;

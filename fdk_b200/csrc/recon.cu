@@ -225,24 +225,31 @@ int flush_all(fdk_recon *h) {
     return FDK_OK;
 }
 
-// Filter n raw views (device) into the filling batch behind the views already there; a full
-// batch is held until the next one starts (rotate_full).  FP32_EXACT: views join a batch only
-// when they continue the waiting views (first == the next view expected); otherwise everything
-// waiting is backprojected first.  Staged precisions: any views join.
-int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cudaEvent_t release) {
+// Filter n raw views (device, consecutive in memory) with view indices ids[0..n) into the
+// filling batch behind the views already there; a full batch is held until the next one starts
+// (rotate_full).  FP32_EXACT: views join a batch only when they continue the waiting views (the
+// next view expected); otherwise everything waiting is backprojected first.  Staged precisions:
+// any views join.
+int process_chunk(fdk_recon *h, const float *d_src, const int64_t *ids, int n, cudaEvent_t release) {
     const fdk_geometry &g = h->g;
     const long long frame = g.nu * g.nv;
     const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
     const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
-    if (h->precision == FDK_BP_FP32_EXACT && (h->pending > 0 || h->held)) {
-        const long long expected = h->pending > 0 ? (long long)h->bviews[h->cur].back() + 1
-                                                  : (long long)h->bviews[h->cur ^ 1].back() + 1;
-        if (first != expected) FDK_TRY(flush_all(h));
-    }
+    const bool exact = h->precision == FDK_BP_FP32_EXACT;
     for (int done = 0; done < n;) {
+        if (exact && (h->pending > 0 || h->held)) {
+            const long long expected = h->pending > 0 ? (long long)h->bviews[h->cur].back() + 1
+                                                      : (long long)h->bviews[h->cur ^ 1].back() + 1;
+            if (ids[done] != expected) FDK_TRY(flush_all(h));
+        }
         if (h->pending == h->batch) FDK_TRY(rotate_full(h));
-        const int m = std::min(n - done, h->batch - h->pending);
-        for (int i = 0; i < m; i++) h->bviews[h->cur].push_back((int)(first + done + i));
+        int m = std::min(n - done, h->batch - h->pending);
+        if (exact) {  // one consecutive run at a time
+            int r = 1;
+            while (r < m && ids[done + r] == ids[done + r - 1] + 1) r++;
+            m = r;
+        }
+        for (int i = 0; i < m; i++) h->bviews[h->cur].push_back((int)ids[done + i]);
         void *dst = static_cast<unsigned char *>(h->d_filt[h->cur]) + (size_t)h->pending * dstride * esz;
         std::pair<cudaEvent_t, cudaEvent_t> t;  // filter time only (the flush below is the BP's)
         FDK_CUDA(cudaEventCreate(&t.first));
@@ -265,6 +272,42 @@ int process_chunk(fdk_recon *h, const float *d_src, long long first, int n, cuda
     // the raw views are consumed once filtered
     if (release) FDK_CUDA(cudaEventRecord(release, h->compute));
     h->views += n;
+    return FDK_OK;
+}
+
+std::vector<int64_t> consecutive(int64_t first, int64_t n) {
+    std::vector<int64_t> v(n);
+    for (int64_t i = 0; i < n; i++) v[i] = first + i;
+    return v;
+}
+
+// Host views through the copy ring: chunks of up to h->chunk views, each copied into a ring slot
+// on the copy stream and filtered on the compute stream; returns once the last copy has landed.
+int push_host(fdk_recon *h, const float *host_views, const int64_t *ids, int64_t n) {
+    const long long frame = h->g.nu * h->g.nv;
+    const int cap = h->chunk;
+    cudaEvent_t last = nullptr;
+    for (long long c = 0; c < n; c += cap) {
+        const int m = (int)std::min<long long>(cap, n - c);
+        const int k = h->slot;
+        h->slot = (k + 1) % (int)h->d_raw.size();
+        FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
+        FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], host_views + c * frame, sizeof(float) * frame * m,
+                                 cudaMemcpyHostToDevice, h->copy));
+        FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
+        FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
+        FDK_TRY(process_chunk(h, h->d_raw[k], ids + c, m, h->raw_free[k]));
+        last = h->raw_ready[k];
+    }
+    // the caller may reuse host_views once its last copy has landed
+    if (last) FDK_TRY(wait_event(last, "view copy"));
+    return FDK_OK;
+}
+
+int check_ids(const fdk_recon *h, const int64_t *ids, int64_t n) {
+    for (int64_t i = 0; i < n; i++)
+        FDK_CHECK_ARG(ids[i] >= 0 && ids[i] < h->g.n_proj, "view %lld outside 0..%lld", (long long)ids[i],
+                      (long long)h->g.n_proj - 1);
     return FDK_OK;
 }
 
@@ -406,24 +449,19 @@ int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t
                   (long long)first, (long long)(first + n), (long long)h->g.n_proj);
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    const long long frame = h->g.nu * h->g.nv;
-    const int cap = h->chunk;
-    cudaEvent_t last = nullptr;
-    for (long long c = 0; c < n; c += cap) {
-        const int m = (int)std::min<long long>(cap, n - c);
-        const int k = h->slot;
-        h->slot = (k + 1) % (int)h->d_raw.size();
-        FDK_CUDA(cudaStreamWaitEvent(h->copy, h->raw_free[k], 0));
-        FDK_CUDA(cudaMemcpyAsync(h->d_raw[k], host_views + c * frame, sizeof(float) * frame * m,
-                                 cudaMemcpyHostToDevice, h->copy));
-        FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
-        FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
-        FDK_TRY(process_chunk(h, h->d_raw[k], first + c, m, h->raw_free[k]));
-        last = h->raw_ready[k];
-    }
-    // the caller may reuse host_views once its last copy has landed
-    if (last) FDK_TRY(wait_event(last, "view copy"));
-    return FDK_OK;
+    const std::vector<int64_t> ids = consecutive(first, n);
+    return push_host(h, host_views, ids.data(), n);
+    FDK_ABI_END
+}
+
+int fdk_recon_push_views(fdk_recon *h, const float *host_views, const int64_t *views, int64_t n) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && host_views && views && n > 0, "NULL argument or empty list");
+    FDK_TRY(check_ids(h, views, n));
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    return push_host(h, host_views, views, n);
     FDK_ABI_END
 }
 
@@ -476,10 +514,22 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
         FDK_CUDA(cudaEventRecord(h->stage_free[b], h->copy));
         FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
         FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
-        FDK_TRY(process_chunk(h, h->d_raw[k], first + c, m, h->raw_free[k]));
+        const std::vector<int64_t> ids = consecutive(first + c, m);
+        FDK_TRY(process_chunk(h, h->d_raw[k], ids.data(), m, h->raw_free[k]));
     }
     return FDK_OK;
     FDK_ABI_END
+}
+
+// Device views: filtered straight from the caller's memory, batch by batch.
+int push_device_ids(fdk_recon *h, const float *dev_views, const int64_t *ids, int64_t n) {
+    const long long frame = h->g.nu * h->g.nv;
+    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
+    for (long long c = 0; c < n; c += cap) {
+        const int m = (int)std::min<long long>(cap, n - c);
+        FDK_TRY(process_chunk(h, dev_views + c * frame, ids + c, m, nullptr));
+    }
+    return FDK_OK;
 }
 
 int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n) {
@@ -489,13 +539,19 @@ int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, i
     FDK_CHECK_ARG(first >= 0 && n > 0 && first + n <= h->g.n_proj, "view range outside the scan");
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    const long long frame = h->g.nu * h->g.nv;
-    const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
-    for (long long c = 0; c < n; c += cap) {
-        const int m = (int)std::min<long long>(cap, n - c);
-        FDK_TRY(process_chunk(h, dev_views + c * frame, first + c, m, nullptr));
-    }
-    return FDK_OK;
+    const std::vector<int64_t> ids = consecutive(first, n);
+    return push_device_ids(h, dev_views, ids.data(), n);
+    FDK_ABI_END
+}
+
+int fdk_recon_push_device_views(fdk_recon *h, const float *dev_views, const int64_t *views, int64_t n) {
+    FDK_ABI_BEGIN
+    clear_error();
+    FDK_CHECK_ARG(h && dev_views && views && n > 0, "NULL argument or empty list");
+    FDK_TRY(check_ids(h, views, n));
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    return push_device_ids(h, dev_views, views, n);
     FDK_ABI_END
 }
 

@@ -44,6 +44,21 @@ class Reconstructor:
     def push_ptr(self, host_ptr: int, first: int, n: int) -> None:
         check(lib().fdk_recon_push(self._h, host_ptr, first, n))
 
+    def push_views(self, views: np.ndarray, ids) -> None:
+        """Raw views (n, nv, nu) float32 in host memory with view indices ids (any order)."""
+        if views.dtype != np.float32 or not views.flags.c_contiguous:
+            raise ValueError("views must be C-contiguous float32")
+        self.push_views_ptr(views.ctypes.data, ids)
+
+    def push_views_ptr(self, host_ptr: int, ids) -> None:
+        ids = np.ascontiguousarray(ids, np.int64)
+        check(lib().fdk_recon_push_views(self._h, host_ptr, ids.ctypes.data, len(ids)))
+
+    def push_device_views(self, dev_ptr: int, ids) -> None:
+        """Raw views in device memory, one after another, with view indices ids (any order)."""
+        ids = np.ascontiguousarray(ids, np.int64)
+        check(lib().fdk_recon_push_device_views(self._h, dev_ptr, ids.ctypes.data, len(ids)))
+
     @property
     def filter_kind(self) -> str:
         """'fft' or 'tensor' (the split-FP16 tcgen05 GEMM filter)."""

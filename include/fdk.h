@@ -274,6 +274,13 @@ int fdk_recon_stream(fdk_recon *h, void **stream);
 int fdk_recon_push(fdk_recon *h, const float *host_views, int64_t first, int64_t n);
 /* Push n raw views already in device memory (nv x nu each). */
 int fdk_recon_push_device(fdk_recon *h, const float *dev_views, int64_t first, int64_t n);
+/* No counterpart in the reference.  Push n raw views whose indices are views[0..n) (any order,
+ * each in 0..n_proj-1), stored one after another in host_views (pinned memory overlaps best) or
+ * dev_views: one copy and one filter launch for views the caller reads out of order, e.g. a few
+ * consecutive views from each quarter of the scan, so that the quarter-turn kernel
+ * (fdk_recon_bp_kernel) finds whole orbits in every batch.  Returns as fdk_recon_push. */
+int fdk_recon_push_views(fdk_recon *h, const float *host_views, const int64_t *views, int64_t n);
+int fdk_recon_push_device_views(fdk_recon *h, const float *dev_views, const int64_t *views, int64_t n);
 /* Push views first..first+n-1 from a projection folder (files as fdk_proj_path, view v in file
  * v * step + start).  Files are read by `threads` host threads (<= 0: up to 8) into two pinned
  * staging buffers of one batch each, so reading batch k+1 overlaps the copy and the kernels of

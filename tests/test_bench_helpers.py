@@ -24,13 +24,23 @@ def test_step_chunks_read_every_view_once_in_quarter_order():
     import fdk_b200 as F
 
     p = F.config("c3")
-    seen = sorted(v for b in range(128) for f, n in bench.step_chunks(p, b) for v in range(f, f + n))
+    seen = sorted(v for b in range(128) for f, n in bench.step_chunks(p, b, order="quarter") for v in range(f, f + n))
     assert seen == list(range(4096))
     # each step: 8 views from each quarter, partners v + k N/4 in the same step
-    ch = bench.step_chunks(p, 3)
+    ch = bench.step_chunks(p, 3, order="quarter")
     assert [n for _, n in ch] == [8] * 4 and [f - ch[0][0] for f, _ in ch] == [0, 1024, 2048, 3072]
     # a scan whose quarter does not split into 8-view chunks reads 32 consecutive views
-    assert bench.step_chunks(F.config("c5"), 2) == [(64, 32)]
+    assert bench.step_chunks(F.config("c5"), 2, order="quarter") == [(64, 32)]
+    assert bench.step_chunks(p, 3, order="sequential") == [(96, 32)]
+
+
+def test_read_order_follows_the_pairing(monkeypatch):
+    import fdk_b200 as F
+
+    monkeypatch.delenv("FDK_BP_SYM", raising=False)
+    assert bench.pairs_views(F.config("c3"), "fp32") and not bench.pairs_views(F.config("c3"), "mixed")
+    monkeypatch.setenv("FDK_BP_SYM", "1")
+    assert bench.pairs_views(F.config("c3"), "mixed") and not bench.pairs_views(F.config("c5"), "mixed")
 
 
 class _Done:
