@@ -489,26 +489,44 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     peaks = F._lib.probe_peaks(local)
     log(f"probes: {peaks}")
     # ---- inputs resident in HBM: exact projections of the seeded phantom, in step order (step
-    # b's chunks, step_chunks(), one after another; steps beyond the pool reuse it cyclically)
+    # b's chunks, step_chunks(), one after another; steps beyond the pool reuse it cyclically).
+    # Each leg reads in the order its reconstructor runs best (READ_ORDER for the timed
+    # precision); a pool in another order is generated when a leg needs one.
     ell = P.phantom_for(param, 3, 30)
-    views = torch.empty((n_dev_views, param.nv, param.nu), dtype=torch.float32, device="cuda")
-    for b in range(pool_steps):
-        o = b * B
-        for first, n in step_chunks(param, b):
-            P.project(param, ell, first, n, views[o:].data_ptr())
-            o += n
-    torch.cuda.synchronize()
-    log(f"generated {n_dev_views} views ({n_dev_views * frame * 4 / GIB:.1f} GiB) in HBM")
+    pools = {}
 
-    def chunks_of(b):
+    def pool(order):
+        if order not in pools:
+            for k in list(pools):  # one pool at a time on the device
+                del pools[k]
+            torch.cuda.empty_cache()
+            v = torch.empty((n_dev_views, param.nv, param.nu), dtype=torch.float32, device="cuda")
+            for b in range(pool_steps):
+                o = b * B
+                for first, n in step_chunks(param, b, order=order):
+                    P.project(param, ell, first, n, v[o:].data_ptr())
+                    o += n
+            torch.cuda.synchronize()
+            pools[order] = v
+            log(f"generated {n_dev_views} views ({n_dev_views * frame * 4 / GIB:.1f} GiB, {order} order) in HBM")
+        return pools[order]
+
+    def chunks_of(b, order=None):
         """Step b's push: (device pointer of its B views in the pool, their view indices)."""
-        ids = np.array([v for first, n in step_chunks(param, b) for v in range(first, first + n)], np.int64)
-        return views[(b % pool_steps) * B:].data_ptr(), ids
+        order = order or READ_ORDER
+        ids = np.array([v for first, n in step_chunks(param, b, order=order) for v in range(first, first + n)],
+                       np.int64)
+        return pool(order)[(b % pool_steps) * B:].data_ptr(), ids
 
-    def timed_device_run(precision: str, steps: int, warmup: int):
+    def order_of(precision):
+        return "quarter" if pairs_views(param, precision) else "sequential"
+
+    def timed_device_run(precision: str, steps: int, warmup: int, order=None):
+        order = order or READ_ORDER
+        pool(order)
         r = F.Reconstructor(param, precision, batch=BATCH, device=local, slab=slab)
         for b in range(warmup):
-            r.push_device_views(*chunks_of(b))
+            r.push_device_views(*chunks_of(b, order))
         r.sync()
         st0 = r.stats()
         l0 = r.launch_count
@@ -517,7 +535,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for b in range(warmup, warmup + steps):
-            r.push_device_views(*chunks_of(b))
+            r.push_device_views(*chunks_of(b, order))
         r.flush()  # backproject a last partial batch inside the timed region
         e1.record(stream)
         e1.synchronize()
@@ -548,25 +566,27 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
     # ---- plain FP32: the same timed run (same steps and warm-up) in FP32
     fp32 = None
     if not args.no_compare and args.precision == "mixed":
-        r2, ms2, bp2, _, _ = timed_device_run("fp32", args.steps, args.warmup)
+        r2, ms2, bp2, _, _ = timed_device_run("fp32", args.steps, args.warmup, order_of("fp32"))
+        fp32_kind = r2.bp_kernel
         r2.close()
         del r2
         torch.cuda.empty_cache()
         v2 = upd_step_all * args.steps / (allmax(ms2) * 1e-3) / 1e9
         fp32 = {"value": v2, "unit": "GUPS", "steps": args.steps, "warmup": args.warmup,
                 "bp_kernel_gups": upd_step_rank * args.steps / (bp2 * 1e-3) / 1e9,
-                "speedup_mixed_over_fp32": value / v2}
+                "speedup_mixed_over_fp32": value / v2, "bp_kernel": fp32_kind, "read_order": order_of("fp32")}
         log(f"fp32: {fp32}")
 
     # ---- accuracy at full size against the FP64 oracle (rank 0; the checker, not timed)
     acc = None
     if not args.no_compare and rank == 0:
-        acc = accuracy_leg(F, param, views, chunks_of, min(args.steps, pool_steps), slab, local, log)
+        acc = accuracy_leg(F, param, pool("quarter"), lambda b: chunks_of(b, "quarter"), min(args.steps, pool_steps),
+                           slab, local, log)
 
     # ---- the reference's own GPU backprojector beside ours (rank 0, N = 1)
     ref_gpu = None
     if not args.no_compare and rank == 0 and world == 1 and param.nu == 2048 and param.nx == 2048:
-        ref_gpu = reference_gpu_leg(F, param, views, chunks_of, local, log)
+        ref_gpu = reference_gpu_leg(F, param, pool("quarter"), lambda b: chunks_of(b, "quarter"), local, log)
 
     # ---- end to end through the public API with host buffers
     e2e = None
@@ -575,19 +595,19 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
 
         vol_bytes = param.nx * param.ny * 2 * slab[1] * 4
         avail = psutil.virtual_memory().available / max(1, world)
-        pool = int(min(n_dev_views, max(64, (avail * 0.6 - vol_bytes) // (frame * 4))))
-        pool = max(B, (pool // B) * B)  # whole steps of the device pool's step order
-        host_views = torch.empty((pool, param.nv, param.nu), dtype=torch.float32, pin_memory=True)
-        host_views.copy_(views[:pool])
+        pool_n = int(min(n_dev_views, max(64, (avail * 0.6 - vol_bytes) // (frame * 4))))
+        pool_n = max(B, (pool_n // B) * B)  # whole steps of the device pool's step order
+        host_views = torch.empty((pool_n, param.nv, param.nu), dtype=torch.float32, pin_memory=True)
+        host_views.copy_(pool(READ_ORDER)[:pool_n])
         host_vol = None
-        if avail * 0.8 > vol_bytes + pool * frame * 4:
+        if avail * 0.8 > vol_bytes + pool_n * frame * 4:
             host_vol = torch.empty(param.nx * param.ny * 2 * slab[1], dtype=torch.float32, pin_memory=True)
-        del views
+        pools.clear()
         torch.cuda.empty_cache()
-        host_steps = pool // B
+        host_steps = pool_n // B
 
         def host_step(b):
-            ids = np.array([v for first, n in step_chunks(param, b % pool_steps) for v in range(first, first + n)],
+            ids = np.array([v for first, n in step_chunks(param, b % host_steps) for v in range(first, first + n)],
                            np.int64)
             return host_views[(b % host_steps) * B:].data_ptr(), ids
 
@@ -609,10 +629,10 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         e2e = {"value": upd_step_all * args.steps / te / 1e9, "unit": "GUPS",
                "h2d_bytes_per_step": B * frame * 4,
                "d2h_bytes_per_step": (vol_bytes // args.steps) if host_vol is not None else 4,
-               "seconds": te, "host_pool_views": pool,
+               "seconds": te, "host_pool_views": pool_n,
                "note": ("the whole volume is read back once at the end, counted per step; "
                         + ("host views are a pinned pool of the workload's views reused cyclically"
-                           if pool < param.nProj else "all views from pinned host memory"))}
+                           if pool_n < param.nProj else "all views from pinned host memory"))}
         log(f"e2e: {e2e}")
         re.close()
 
