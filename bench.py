@@ -620,6 +620,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         t0 = time.perf_counter()
         for b in range(args.steps):
             re.push_views_ptr(*host_step(b))
+        t_push = time.perf_counter() - t0
         if host_vol is not None:
             re.volume_into(host_vol.data_ptr())
         else:
@@ -629,7 +630,7 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         e2e = {"value": upd_step_all * args.steps / te / 1e9, "unit": "GUPS",
                "h2d_bytes_per_step": B * frame * 4,
                "d2h_bytes_per_step": (vol_bytes // args.steps) if host_vol is not None else 4,
-               "seconds": te, "host_pool_views": pool_n,
+               "seconds": te, "push_seconds": t_push, "host_pool_views": pool_n,
                "note": ("the whole volume is read back once at the end, counted per step; "
                         + ("host views are a pinned pool of the workload's views reused cyclically"
                            if pool_n < param.nProj else "all views from pinned host memory"))}
