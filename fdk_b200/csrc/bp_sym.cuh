@@ -220,9 +220,10 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
     using C = SymCfg<E>;
     constexpr int R = C::R;
     constexpr unsigned BOX = sym_box_bytes<E>();
-    const float *m = md.m;
-    const bool interior = md.interior;  // read once: md lives in shared memory
-    const int u_lo = md.u_lo, v_lo = md.v_lo;
+    const MetaRegs mr = load_meta(md);  // md lives in shared memory: four 128-bit loads
+    const float *m = mr.m;
+    const bool interior = mr.interior;
+    const int u_lo = mr.u_lo, v_lo = mr.v_lo;
     const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
     const float rw = __fdividef(1.0f, w);
     const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;

@@ -29,6 +29,7 @@
 #include <cuda.h>
 #include <cuda_fp16.h>
 
+#include <cstddef>
 #include <type_traits>
 
 #include "common.h"
@@ -86,6 +87,7 @@ struct __align__(16) TmaMeta {
     int u_lo, v_lo, staged;
     int interior;  // every detector row v of the tile's voxels lies inside (0, nv-1): no per-slice checks
 };
+static_assert(sizeof(TmaMeta) == 64 && offsetof(TmaMeta, u_lo) == 48, "load_meta reads TmaMeta as 4 x 16 B");
 
 struct BpTmaArgs {
     float *vol;
@@ -167,6 +169,33 @@ __device__ __forceinline__ void acc_add_f16x2(float &lo_acc, float &hi_acc, __ha
         : "r"(u));
 }
 
+// A view's metadata in registers, read from shared memory with four 128-bit loads (the struct is
+// 16-byte aligned: m[0..3], m[4..7], m[8..11], then u_lo, v_lo, staged, interior) instead of up
+// to sixteen scalar ones per column and view.
+#ifndef FDK_META_SCALAR
+#define FDK_META_SCALAR 0
+#endif
+struct MetaRegs {
+    float m[12];
+    int u_lo, v_lo, staged, interior;
+};
+__device__ __forceinline__ MetaRegs load_meta(const TmaMeta &md) {
+#if FDK_META_SCALAR  // tuning comparison: field by field
+    MetaRegs r;
+    for (int i = 0; i < 12; i++) r.m[i] = md.m[i];
+    r.u_lo = md.u_lo;
+    r.v_lo = md.v_lo;
+    r.staged = md.staged;
+    r.interior = md.interior;
+    return r;
+#endif
+    const float4 a = *reinterpret_cast<const float4 *>(&md.m[0]);
+    const float4 b = *reinterpret_cast<const float4 *>(&md.m[4]);
+    const float4 c = *reinterpret_cast<const float4 *>(&md.m[8]);
+    const int4 d = *reinterpret_cast<const int4 *>(&md.u_lo);
+    return MetaRegs{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w}, d.x, d.y, d.z, d.w};
+}
+
 // Footprint box of a tile in one view; fills meta (matrix copied by the caller).
 template <typename E>
 __device__ __forceinline__ void tile_box(const float *m, float xa, float xb, float ya, float yb, float za, float zb,
@@ -199,11 +228,12 @@ __device__ __forceinline__ void tile_box(const float *m, float xa, float xb, flo
 
 // One view's contribution to a thread's column: R voxel pairs.
 template <typename E>
-__device__ __forceinline__ void column_view(const TmaMeta &md, unsigned box, const E *gview, float x, float y,
+__device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, const E *gview, float x, float y,
                                             float zf0, int nu, int nv, float wscale, float (&am)[TmaCfg<E>::R],
                                             float (&ar)[TmaCfg<E>::R]) {
     using C = TmaCfg<E>;
     constexpr int R = C::R;
+    const MetaRegs md = load_meta(md_s);
     const float *m = md.m;
     const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
     const float rw = __fdividef(1.0f, w);
