@@ -206,6 +206,18 @@ struct fdk_bp {
     unsigned int *h_err = nullptr;            // pinned host copy of the device error word
     int sym_rot = 0;                          // quarter-turn kernel: its column map (0: not set up)
     int sym_ctas = 0;                         // its persistent grid
+    // Ring of launch view lists (fdk_bp_bp_lists_internal): a pinned host record per entry,
+    // uploaded on the launch stream to the entry's device copy, which the kernel reads; an entry
+    // is written again once the event recorded after its launch has passed.
+    union ListRec {
+        SymQuads quads;
+        ViewList views;
+    };
+    static constexpr int kListRing = 64;
+    ListRec *h_list = nullptr, *d_list = nullptr;
+    cudaEvent_t list_ev[kListRing] = {};
+    bool list_used[kListRing] = {};
+    int list_next = 0;
 };
 
 namespace bpi {
@@ -540,6 +552,12 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
                                               : tma_prepare<float2>(h->plan.tma_ctas, device);
                 if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
                 if (s == FDK_OK) ck(cudaMemsetAsync(h->plan.d_err, 0, sizeof(unsigned int), h->stream), "error word");
+                if (s == FDK_OK)
+                    ck(cudaHostAlloc((void **)&h->h_list, sizeof(fdk_bp::ListRec) * fdk_bp::kListRing, 0), "view lists");
+                if (s == FDK_OK)
+                    ck(cudaMalloc(&h->d_list, sizeof(fdk_bp::ListRec) * fdk_bp::kListRing), "view lists");
+                for (int i = 0; i < fdk_bp::kListRing && s == FDK_OK; i++)
+                    ck(cudaEventCreateWithFlags(&h->list_ev[i], cudaEventDisableTiming), "event");
             }
         }
     }
@@ -581,6 +599,20 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         ck(cudaEventCreateWithFlags(&h->band_done[k], cudaEventDisableTiming), "event");
     for (int i = 0; i < 2 && s == FDK_OK; i++)
         ck(cudaStreamCreateWithFlags(&h->rb[i], cudaStreamNonBlocking), "readback stream");
+    if (s == FDK_OK) {
+        // Load the kernels that run beside a backprojection now.  With lazy module loading (the
+        // CUDA 12 default) a kernel's code is loaded at its first launch, and that load waits for
+        // the device to go idle: a first readback issued beside the last batch waited for all of
+        // its backprojection (measured: the volume returned 0.6 s after the last band instead of
+        // overlapping the bands), and so would a first view conversion beside a batch.
+        cudaFuncAttributes fa;
+        const void *kernels[] = {(const void *)transform_volume_kernel<true>,
+                                 (const void *)transform_volume_kernel<false>, (const void *)absmax_kernel,
+                                 (const void *)to_mirror_half_kernel, (const void *)to_mirror_kernel<float2>,
+                                 (const void *)fold_comp_kernel};
+        for (const void *kf : kernels)
+            if (s == FDK_OK) ck(cudaFuncGetAttributes(&fa, kf), "kernel load");
+    }
     if (s == FDK_OK) {
         // readback staging: two buffers of whole 32-plane tiles (32 planes, or about 128 MB where
         // planes are small), allocated here so that a readback never calls the allocator while
@@ -809,6 +841,13 @@ int fdk_bp_destroy(fdk_bp *h) {
                 cudaStreamDestroy(h->rb[i]);
             }
         if (h->d_rb) cudaFree(h->d_rb);
+        for (int i = 0; i < fdk_bp::kListRing; i++)
+            if (h->list_ev[i]) {
+                if (h->list_used[i]) wait_event(h->list_ev[i], "view list");  // its upload has been read
+                cudaEventDestroy(h->list_ev[i]);
+            }
+        if (h->h_list) cudaFreeHost(h->h_list);
+        if (h->d_list) cudaFree(h->d_list);
         for (int i = 0; i < 3; i++)
             if (h->sync_ev[i]) cudaEventDestroy(h->sync_ev[i]);
         if (h->h_err) cudaFreeHost(h->h_err);
@@ -904,6 +943,28 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
     return FDK_OK;
 }
 
+namespace {
+// The next entry of the handle's list ring, once the launch that last read it has finished (a
+// bounded wait; immediate unless the host runs kListRing launches ahead of the device).
+int take_list(fdk_bp *h, fdk_bp::ListRec **rec, fdk_bp::ListRec **dev, int *entry) {
+    FDK_CHECK_ARG(h->h_list && h->d_list, "no view-list ring (staged precisions only)");
+    const int i = h->list_next;
+    h->list_next = (i + 1) % fdk_bp::kListRing;
+    if (h->list_used[i]) FDK_TRY(wait_event(h->list_ev[i], "view list"));
+    h->list_used[i] = false;
+    *rec = h->h_list + i;
+    *dev = h->d_list + i;
+    *entry = i;
+    return FDK_OK;
+}
+// Entry i is busy until the work queued on st so far (its upload and launch) has finished.
+int release_list(fdk_bp *h, int i, cudaStream_t st) {
+    FDK_CUDA(cudaEventRecord(h->list_ev[i], st));
+    h->list_used[i] = true;
+    return FDK_OK;
+}
+}  // namespace
+
 // One batch of views held in a device views buffer (n_slots views, any order), for the
 // reconstructor (recon.cu): `n_single` views by (slot, view) through the staged kernel and
 // `n_quad` quarter-turn quadruples (4 slots each, members b, b + N/4, b + N/2, b + 3N/4 mod N, and
@@ -930,39 +991,65 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
     std::pair<cudaEvent_t, cudaEvent_t> tm;
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
-    static thread_local SymQuads sq;
-    static thread_local ViewList vl;
     for (int k = kb; k < ke; k++) {
         for (int q0 = 0; q0 < n_quad; q0 += kSymMaxQuads) {
             const int nq = std::min(kSymMaxQuads, n_quad - q0);
+            fdk_bp::ListRec *rec = nullptr, *dev = nullptr;
+            int e = 0;
+            FDK_TRY(take_list(h, &rec, &dev, &e));
+            SymQuads &sq = rec->quads;
             for (int i = 0; i < nq; i++) {
                 const int *s4 = q_slot + 4 * (q0 + i);
                 sq.slot[i] = make_int4(s4[0], s4[1], s4[2], s4[3]);
                 sq.view[i] = q_view[q0 + i];
             }
-            if (mixed)
-                FDK_TRY(bp_sym_launch<__half2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots, d_mats,
-                                               host_mats, sq, nq, h->sym_rot, st, acc_scale, h->band_z[k],
-                                               h->band_z[k + 1]));
-            else
-                FDK_TRY(bp_sym_launch<float2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots, d_mats,
-                                              host_mats, sq, nq, h->sym_rot, st, acc_scale, h->band_z[k],
-                                              h->band_z[k + 1]));
+            FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(SymQuads), cudaMemcpyHostToDevice, st));
+            const int r = mixed ? bp_sym_launch<__half2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots,
+                                                         d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
+                                                         acc_scale, h->band_z[k], h->band_z[k + 1])
+                                : bp_sym_launch<float2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots,
+                                                        d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
+                                                        acc_scale, h->band_z[k], h->band_z[k + 1]);
+            FDK_TRY(release_list(h, e, st));
+            FDK_TRY(r);
             h->launches++;
         }
         for (int s0 = 0; s0 < n_single; s0 += kMaxListViews) {
             const int ns = std::min(kMaxListViews, n_single - s0);
+            bool run = s_slot[s0] >= 0 && s_slot[s0] + ns <= n_slots;
+            for (int i = 1; i < ns && run; i++)
+                run = s_slot[s0 + i] == s_slot[s0] + i && s_view[s0 + i] == s_view[s0] + i;
+            if (run) {
+                // consecutive views in consecutive slots: a launch without a list, over the
+                // buffer from the run's first slot (the kernel's loop then reads no list)
+                const size_t frame = (size_t)h->plan.nu * h->plan.nv * (mixed ? sizeof(__half2) : sizeof(float2));
+                const void *pv = static_cast<const char *>(views) + frame * s_slot[s0];
+                const long long m0 = 12 * (long long)s_view[s0];
+                FDK_TRY(mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                                                       ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
+                              : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                                                      ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                h->launches++;
+                continue;
+            }
+            fdk_bp::ListRec *rec = nullptr, *dev = nullptr;
+            int e = 0;
+            FDK_TRY(take_list(h, &rec, &dev, &e));
+            ViewList &vl = rec->views;
             vl.n = ns;
             for (int i = 0; i < ns; i++) {
                 vl.slot[i] = s_slot[s0 + i];
                 vl.view[i] = s_view[s0 + i];
             }
-            if (mixed)
-                FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st, acc_scale,
-                                               h->band_tz[k], h->band_tz[k + 1], &vl, n_slots));
-            else
-                FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st, acc_scale,
-                                              h->band_tz[k], h->band_tz[k + 1], &vl, n_slots));
+            FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(ViewList), cudaMemcpyHostToDevice, st));
+            const int r = mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
+                                                         acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
+                                                         n_slots)
+                                : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
+                                                        acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
+                                                        n_slots);
+            FDK_TRY(release_list(h, e, st));
+            FDK_TRY(r);
             h->launches++;
         }
         FDK_CUDA(cudaEventRecord(h->band_done[k], st));

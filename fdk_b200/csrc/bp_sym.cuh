@@ -116,7 +116,7 @@ struct SymCfg<float2> {
 
 constexpr int kSymMaxQuads = 512;
 
-// Quadruples of one launch (kernel parameter, 10 KB): the slots (views-buffer index, the TMA z
+// Quadruples of one launch (a host record, uploaded to a device copy that the kernel reads): the slots (views-buffer index, the TMA z
 // coordinate) of the four members b, b + N/4, b + N/2, b + 3N/4 (mod N), and the base view b
 // whose matrix the four share.  A batch with whole orbits lists each view once as the base, so
 // every view reaches every column: base columns c through itself, T^j(c) through the quadruple
@@ -143,6 +143,8 @@ struct BpSymArgs {
     int rot;             // quarter turn: > 0 T(x, y) = (y, n-1-x), < 0 T(x, y) = (n-1-y, x)
     unsigned long long wait_ns;
     int withhold;        // test switch (FDK_BP_TEST_WITHHOLD): CTA 0 never fills its first stage
+    const int4 *q_slot;  // device copy of the launch's quadruples: n_quads slots and base views
+    const int *q_view;
 };
 
 // Volume offset ([x][y][zs]) of column T^j(x, y), T the launch's quarter turn.
@@ -332,7 +334,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
 #endif
 template <typename E>
 __global__ void __maxnreg__(FDK_SYM_MAXNREG)
-    bp_sym_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ SymQuads q, BpSymArgs a) {
+    bp_sym_kernel(const __grid_constant__ CUtensorMap tmap, BpSymArgs a) {
     using C = SymCfg<E>;
     constexpr int R = C::R, NQ = C::NQ, S = C::S;
     constexpr int BOX = sym_box_bytes<E>();
@@ -379,7 +381,7 @@ __global__ void __maxnreg__(FDK_SYM_MAXNREG)
                 if (lane < NQ) {
                     TmaMeta &md = meta[s * NQ + lane];
                     if (qd < a.n_quads) {
-                        const float *mg = a.mats + 12 * (long long)q.view[qd];
+                        const float *mg = a.mats + 12 * (long long)__ldg(a.q_view + qd);
 #pragma unroll
                         for (int i = 0; i < 12; i++) md.m[i] = __ldg(mg + i);
                         sym_tile_box<E>(md.m, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
@@ -402,7 +404,7 @@ __global__ void __maxnreg__(FDK_SYM_MAXNREG)
                         const int ql = c * NQ + l;
                         const TmaMeta &md = meta[s * NQ + l];
                         if (ql < a.n_quads && md.staged) {
-                            const int4 sl = q.slot[ql];
+                            const int4 sl = __ldg(a.q_slot + ql);
                             const unsigned dst = boxes + (s * NQ + l) * 4 * BOX;
                             tma_load_3d(dst, &tmap, md.v_lo, md.u_lo, sl.x, full0 + 8 * s);
                             tma_load_3d(dst + BOX, &tmap, md.v_lo, md.u_lo, sl.y, full0 + 8 * s);
@@ -513,11 +515,12 @@ inline int sym_prepare(int &ctas, int device) {
 
 // Backproject nq quadruples (slots into a views buffer of n_slots views, base views' matrices in
 // d_mats / host_mats indexed by view) into the top slices [z_begin, z_end) of the slab pair and
-// their mirrors.  The plan's sub-volume must be the whole square x-y grid.
+// their mirrors.  The plan's sub-volume must be the whole square x-y grid.  q: the host record,
+// checked here; d_q: its device copy, which the kernel reads (uploaded on st before this launch).
 template <typename E>
 inline int bp_sym_launch(const BpFastPlan &p, int ctas, float *vol, float *comp, const void *views, int n_slots,
-                         const float *d_mats, const float *host_mats, const SymQuads &q, int nq, int rot,
-                         cudaStream_t st, const float *scale, long long z_begin, long long z_end) {
+                         const float *d_mats, const float *host_mats, const SymQuads &q, const SymQuads *d_q, int nq,
+                         int rot, cudaStream_t st, const float *scale, long long z_begin, long long z_end) {
     using C = SymCfg<E>;
     FDK_CHECK_ARG(((uintptr_t)views & 15) == 0, "TMA views must start on a 16-byte boundary");
     FDK_CHECK_ARG(nq > 0 && nq <= kSymMaxQuads, "quadruples %d outside 1..%d", nq, kSymMaxQuads);
@@ -557,10 +560,14 @@ inline int bp_sym_launch(const BpFastPlan &p, int ctas, float *vol, float *comp,
     a.rot = rot;
     a.wait_ns = bp_wait_ns();
     a.withhold = bp_test_withhold();
+    FDK_CHECK_ARG(d_q != nullptr, "quadruples need their device copy");
+    const char *dq = reinterpret_cast<const char *>(d_q);  // addresses inside the device copy
+    a.q_slot = reinterpret_cast<const int4 *>(dq + offsetof(SymQuads, slot));
+    a.q_view = reinterpret_cast<const int *>(dq + offsetof(SymQuads, view));
     const long long n_tiles = (long long)a.tiles_q * a.tiles_q * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, ctas);
-    bp_sym_kernel<E><<<grid, 288, sym_smem_bytes<E>(), st>>>(map, q, a);
+    bp_sym_kernel<E><<<grid, 288, sym_smem_bytes<E>(), st>>>(map, a);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
 }

@@ -104,11 +104,15 @@ struct BpTmaArgs {
     int tz0;  // first z tile of this launch (a launch may cover a band of z tiles)
     unsigned long long wait_ns;  // limit of every mbarrier wait (FDK_BP_WAIT_NS, default 10 s)
     int withhold;  // test switch (FDK_BP_TEST_WITHHOLD): CTA 0 never fills its first stage
+    // views taken from a views buffer in any order (device arrays of n_proj entries): the slot of
+    // each (the TMA z coordinate) and its view index (its matrix); null: views 0..n_proj-1 in
+    // slots 0..n_proj-1
+    const int *list_slot;
+    const int *list_view;
 };
 
-// Views of one launch taken from a views buffer in any order (kernel parameter): the slot of
-// each (the TMA z coordinate) and its view index (its matrix).  n == 0: views 0..n_proj-1 in
-// slots 0..n_proj-1.
+// Host record of one launch's view list, uploaded to a device copy that the kernel reads (a
+// list passed by value would make the kernel parameters exceed 4 KB).
 constexpr int kMaxListViews = 512;
 struct ViewList {
     int n;
@@ -445,7 +449,7 @@ template <typename E>
 #define FDK_TMA_MIN_BLOCKS 2
 #endif
 __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
-    bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ ViewList vl, BpTmaArgs a) {
+    bp_tma_kernel(const __grid_constant__ CUtensorMap tmap, BpTmaArgs a) {
     using C = TmaCfg<E>;
     constexpr int R = C::R, NV = C::NV, S = C::S;
     constexpr int BOX = tma_box_bytes<E>();
@@ -492,7 +496,7 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
                 if (lane < NV) {
                     TmaMeta &md = meta[s * NV + lane];
                     if (view < a.n_proj) {
-                        const float *mg = a.mats + 12 * (long long)(vl.n ? vl.view[view] : view);
+                        const float *mg = a.mats + 12 * (long long)(a.list_view ? __ldg(a.list_view + view) : view);
 #pragma unroll
                         for (int q = 0; q < 12; q++) md.m[q] = __ldg(mg + q);
                         tile_box<E>(md.m, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
                         const TmaMeta &md = meta[s * NV + l];
                         if (c * NV + l < a.n_proj && md.staged)
                             tma_load_3d(boxes + (s * NV + l) * BOX, &tmap, md.v_lo, md.u_lo,
-                                        vl.n ? vl.slot[c * NV + l] : c * NV + l, full0 + 8 * s);
+                                        a.list_slot ? __ldg(a.list_slot + c * NV + l) : c * NV + l, full0 + 8 * s);
                     }
                 }
                 __syncwarp();
@@ -555,7 +559,7 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
                 for (int l = 0; l < NV; l++) {
                     const int view = c * NV + l;
                     if (view >= a.n_proj) break;
-                    const long long slot = vl.n ? vl.slot[view] : view;
+                    const long long slot = a.list_slot ? __ldg(a.list_slot + view) : view;
                     column_view<E>(meta[s * NV + l], boxes + (s * NV + l) * BOX, proj + slot * frame, x, y, zf0, a.nu,
                                    a.nv, a.wscale, am, ar);
                 }
@@ -628,15 +632,16 @@ inline float weight_scale(const float *host_mats, float xc, float yc) {
 // Backproject n views into the z tiles [tz_begin, tz_end) of R top slices each (with their
 // mirror slices); tz_end < 0 means through the last tile.
 // list (optional): the n views as slots of a buffer of n_slots views and their view indices
-// (matrices d_mats + 12 * view); without it, views and slots 0..n-1.
+// (matrices d_mats + 12 * view), checked here; d_list: its device copy, which the kernel reads
+// (uploaded on st before this launch).  Without a list, views and slots 0..n-1.
 template <typename E>
 inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const void *proj, const float *d_mats,
                          const float *host_mats, int n, cudaStream_t st, const float *scale, int tz_begin = 0,
-                         int tz_end = -1, const ViewList *list = nullptr, int n_slots = 0) {
+                         int tz_end = -1, const ViewList *list = nullptr, const ViewList *d_list = nullptr,
+                         int n_slots = 0) {
     using C = TmaCfg<E>;
     FDK_CHECK_ARG(((uintptr_t)proj & 15) == 0, "TMA views must start on a 16-byte boundary");
-    static thread_local ViewList identity;  // n = 0
-    identity.n = 0;
+    FDK_CHECK_ARG(!list == !d_list, "a view list needs its device copy");
     if (list) {
         FDK_CHECK_ARG(list->n == n && n <= kMaxListViews, "view list of %d entries for %d views", list->n, n);
         for (int i = 0; i < n; i++)
@@ -672,10 +677,14 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     a.tiles_z = tz_end - tz_begin;
     a.wait_ns = bp_wait_ns();
     a.withhold = bp_test_withhold();
+    // addresses inside the device copy (no host access to it)
+    const char *dl = reinterpret_cast<const char *>(d_list);
+    a.list_slot = d_list ? reinterpret_cast<const int *>(dl + offsetof(ViewList, slot)) : nullptr;
+    a.list_view = d_list ? reinterpret_cast<const int *>(dl + offsetof(ViewList, view)) : nullptr;
     const long long n_tiles = (long long)a.tiles_x * a.tiles_y * a.tiles_z;
     FDK_CHECK_ARG(n_tiles < (1ll << 31), "too many tiles");
     const int grid = (int)std::min<long long>(n_tiles, p.tma_ctas);
-    bp_tma_kernel<E><<<grid, 288, tma_smem_bytes<E>(), st>>>(map, list ? *list : identity, a);
+    bp_tma_kernel<E><<<grid, 288, tma_smem_bytes<E>(), st>>>(map, a);
     FDK_CUDA(cudaGetLastError());
     return FDK_OK;
 }
