@@ -384,6 +384,37 @@ int read_volume(fdk_bp *h, float *host) {
     return FDK_OK;
 }
 
+// z bands: up to kMaxBands launches per batch (FDK_BP_BANDS lowers the cap) when each still
+// gives every CTA of the persistent grid at least 8 tiles (the split costs nothing measurable
+// then).  Boundaries fall on whole `unit`s of slices: the staged kernel's tile height R, or a
+// common multiple of it and the quarter-turn kernel's once that kernel is set up; each boundary
+// is the whole unit nearest an even split of the slices.
+void set_bands(fdk_bp *h, int unit) {
+    const int R = h->precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+    const long long depth = (long long)h->top.depth;
+    const long long cols = ceil_div((long long)h->top.width, 16) * ceil_div((long long)h->top.height, 16);
+    const int tiles_z = (int)ceil_div(depth, R);
+    const int units = (int)ceil_div(depth, unit);
+    const char *cap = getenv("FDK_BP_BANDS");
+    const int max_bands = cap ? std::max(1, std::min(kMaxBands, atoi(cap))) : kMaxBands;
+    int nb = std::min(max_bands, units);
+    while (nb > 1 && cols * (tiles_z / nb) < 8ll * h->plan.tma_ctas) nb--;
+    h->n_bands = nb;
+    for (int k = 0; k <= nb; k++) {
+        h->band_z[k] = std::min<long long>((long long)k * units / nb * unit, depth);
+        if (k > 0 && k < nb) h->band_z[k] = std::min<long long>((k * depth / nb + unit / 2) / unit * unit, depth);
+        h->band_tz[k] = k == nb ? tiles_z : (int)(h->band_z[k] / R);
+    }
+    for (int k = 1; k <= nb; k++)  // rounding must leave no band empty
+        if (h->band_z[k] <= h->band_z[k - 1]) {
+            for (int j = 0; j <= nb; j++) {
+                h->band_z[j] = std::min<long long>((long long)j * units / nb * unit, depth);
+                h->band_tz[j] = j == nb ? tiles_z : (int)(h->band_z[j] / R);
+            }
+            break;
+        }
+}
+
 // The fast kernels need circular-orbit matrices: rows 0 and 2 without a z term.
 int check_circular(const float *mats, int n) {
     for (int i = 0; i < n; i++)
@@ -561,40 +592,10 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             }
         }
     }
-    // z bands: up to kMaxBands launches per batch (FDK_BP_BANDS lowers the cap) when each
-    // still gives every CTA of the persistent grid at least 8 tiles (the split costs nothing
-    // measurable then)
     h->band_z[0] = 0;
     h->band_z[1] = (long long)t.depth;
-    if (s == FDK_OK && h->plan.tma_ok && sym) {
-        const int R = precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
-        // band boundaries fall on whole tiles of both staged kernels (the quarter-turn one too)
-        const int Rs = precision == FDK_BP_MIXED ? SymCfg<__half2>::R : SymCfg<float2>::R;
-        int unit = R;
-        while (unit % Rs) unit += R;
-        const long long cols = ceil_div((long long)t.width, 16) * ceil_div((long long)t.height, 16);
-        const int tiles_z = (int)ceil_div((long long)t.depth, R);
-        const int units = (int)ceil_div((long long)t.depth, unit);
-        const char *cap = getenv("FDK_BP_BANDS");
-        const int max_bands = cap ? std::max(1, std::min(kMaxBands, atoi(cap))) : kMaxBands;
-        int nb = std::min(max_bands, units);
-        while (nb > 1 && cols * (tiles_z / nb) < 8ll * h->plan.tma_ctas) nb--;
-        h->n_bands = nb;
-        for (int k = 0; k <= nb; k++) {
-            h->band_z[k] = std::min<long long>((long long)k * units / nb * unit, (long long)t.depth);
-            if (k > 0 && k < nb)  // nearest whole unit to an even split of the slices
-                h->band_z[k] = std::min<long long>(((long long)k * t.depth / nb + unit / 2) / unit * unit, t.depth);
-            h->band_tz[k] = k == nb ? tiles_z : (int)(h->band_z[k] / R);
-        }
-        for (int k = 1; k <= nb; k++)  // rounding must leave no band empty
-            if (h->band_z[k] <= h->band_z[k - 1]) {
-                for (int j = 0; j <= nb; j++) {
-                    h->band_z[j] = std::min<long long>((long long)j * units / nb * unit, (long long)t.depth);
-                    h->band_tz[j] = j == nb ? tiles_z : (int)(h->band_z[j] / R);
-                }
-                break;
-            }
-    }
+    if (s == FDK_OK && h->plan.tma_ok && sym)
+        set_bands(h, precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R);
     for (int k = 0; k < kMaxBands && s == FDK_OK; k++)
         ck(cudaEventCreateWithFlags(&h->band_done[k], cudaEventDisableTiming), "event");
     for (int i = 0; i < 2 && s == FDK_OK; i++)
@@ -916,6 +917,9 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
     if (mode == "0") return FDK_OK;
     if (h->precision == FDK_BP_FP32_EXACT || !h->plan.tma_ok || !h->sym) return FDK_OK;
     if (h->precision == FDK_BP_MIXED && mode != "1") return FDK_OK;
+    // the set-up moves the z band boundaries: only before the first launch (or after a reset),
+    // so that no readback waits on a band event of launches over the old boundaries
+    if (h->launches > 0) return FDK_OK;
     const BpFastPlan &p = h->plan;
     if (p.x0 != 0 || p.y0 != 0 || p.nxs != p.nys || p.nxs != h->nx || h->nx != h->ny || (p.nxs & 1) || n_proj % 4)
         return FDK_OK;
@@ -938,6 +942,11 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
     FDK_TRY(mixed ? sym_prepare<__half2>(h->sym_ctas, h->device) : sym_prepare<float2>(h->sym_ctas, h->device));
+    // bands on whole tiles of both kernels (set up before the first launch)
+    const int Rt = mixed ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+    int unit = Rt;
+    while (unit % R) unit += Rt;
+    set_bands(h, unit);
     h->sym_rot = r;
     *rot = r;
     return FDK_OK;
