@@ -237,7 +237,7 @@ def run_reference(args, param, rank: int) -> None:
     T.close()
     value = float(statistics.median(vals))
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": 0,
+        "impl": "reference", "metric": metric_name(param, args.precision), "value": value, "unit": "GUPS", "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
         "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded random ellipsoids, exact line integrals)",
@@ -254,6 +254,17 @@ def run_reference(args, param, rank: int) -> None:
 PUSH = 32    # views per step (one filter launch)
 BATCH = 512  # views per backprojection batch (every 16th step); --bp-batch changes it
 METRIC = "FDK GUPS at 2048^3 x 4096 views on 1 B200 (mixed precision, rel-L2 <= 1e-3)"
+L2_BYTES = 126 << 20
+
+
+def metric_name(param, precision: str) -> str:
+    """The headline metric for the 2048^3 / 4096-view MIXED workload; the same wording with the
+    workload's own sizes and precision otherwise."""
+    if (param.nx, param.ny, param.nz, param.nProj) == (2048, 2048, 2048, 4096) and precision == "mixed":
+        return METRIC
+    shape = f"{param.nx}^3" if param.nx == param.ny == param.nz else f"{param.nx}x{param.ny}x{param.nz}"
+    prec = "mixed precision, rel-L2 <= 1e-3" if precision == "mixed" else f"{precision} precision"
+    return f"FDK GUPS at {shape} x {param.nProj} views on 1 B200 ({prec})"
 
 
 READ_ORDER = "quarter"  # set by main(): "quarter" or "sequential"
@@ -300,13 +311,23 @@ def count_bp_batches(firsts, n: int, batch: int | None = None, contiguous: bool 
     return sizes
 
 
+def l2_note(param, precision: str) -> str:
+    """How the timed steps stand to the 126 MB L2: the volume (and the MIXED compensation) is
+    read and written by every batch, so it decides whether a step can hit L2."""
+    views = PUSH * param.nu * param.nv * 4
+    vol = param.nx * param.ny * param.nz * 4 * (2 if precision == "mixed" else 1)
+    sizes = f"{views / 2**20:.0f} MiB views per step, {vol / 2**20:.0f} MiB volume state"
+    if vol > L2_BYTES:
+        return f"inputs larger than L2 ({sizes})"
+    return f"inputs smaller than L2 ({sizes}): L2 not flushed between steps"
+
+
 def workload_config(param, args) -> dict:
     return {"workload": f"FDK {param.nx}x{param.ny}x{param.nz} volume from {param.nProj} views of "
                         f"{param.nu}x{param.nv}, batches of {PUSH} views",
             "volume": [param.nx, param.ny, param.nz], "views": param.nProj, "detector": [param.nu, param.nv],
             "batch": PUSH, "bp_batch": BATCH, "precision": args.precision, "filter": param.str_filter,
-            "l2": f"inputs larger than L2 ({PUSH * param.nu * param.nv * 4 >> 20} MiB views per step, "
-                  f"{param.nx * param.ny * param.nz * 4 >> 30} GiB volume)",
+            "l2": l2_note(param, args.precision),
             "parallelism": f"z-slab pairs x{args.gpus}"}
 
 
@@ -671,6 +692,11 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             hbm_peak, hbm_src = 6650.0, "fallback"
         bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / max(1, len(batch_sizes))
         traffic = read_traffic(f"bp_tma_{args.precision}_c2.md", f"dram_bytes_per_{BATCH}_view_batch_full")
+        if traffic is not None and bp_kind != "staged":
+            traffic = None  # the figure is the staged kernel's
+        nvox = param.nx * param.ny * param.nz
+        if traffic is not None and nvox != 2048 ** 3:
+            traffic *= nvox / 2048 ** 3  # recorded for 2048^3 (scaled by voxel count from a 512^3 capture)
         et = '__half2' if args.precision == 'mixed' else 'float2'
         roofline = {
             "kernel": {"quarter-turn": f"bp_sym_kernel<{et}> (views paired with their quarter-turn partners)",
@@ -678,7 +704,8 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             "bound": "smem" if peak_smem <= peak_fma else "fp32",
             "achieved": kernel_gups, "peak": peak, "unit": "GUPS", "frac": kernel_gups / peak,
             "traffic": traffic,
-            "traffic_unit": f"DRAM bytes per full {BATCH}-view batch (ncu, scaled; see profiles)",
+            "traffic_unit": f"DRAM bytes per full {BATCH}-view batch of this workload (ncu capture at 512^3, "
+                            "scaled by voxel count; see profiles)",
             "peak_source": (f"measured on this GPU by fdk_probe_smem ({peaks['smem_gbs']:.0f} GB/s) / {bpu} B "
                             f"per update and fdk_probe_fma ({peaks['fp32_tflops']:.1f} TFLOP/s) / {fpu} FMA per "
                             "update"),
@@ -713,7 +740,8 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
                            "algorithmic_bytes_per_launch": flt_bytes, "launch_ms": flt_step_ms,
                            "traffic": read_traffic(f"filter_{args.precision}_c2.md", "dram_bytes_per_launch_full")}
         out = {
-            "metric": METRIC, "value": value, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+            "metric": metric_name(param, args.precision), "value": value, "unit": "GUPS", "n_gpus": world,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f16" if args.precision == "mixed" else "f32",
             "data": "synthetic: exact line integrals of a seeded 30-ellipsoid phantom (seed 3)",

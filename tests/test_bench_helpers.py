@@ -65,3 +65,15 @@ def test_clock_parser_reads_median_max_and_reasons():
 
 def test_clock_parser_without_nvidia_smi():
     assert bench.ClockSampler(0).stop()["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_metric_and_l2_note_follow_the_workload():
+    import fdk_b200 as F
+
+    c3, c1 = F.config("c3"), F.config("c1")
+    assert bench.metric_name(c3, "mixed") == bench.METRIC
+    assert bench.metric_name(c1, "mixed").startswith("FDK GUPS at 256^3 x 256 views")
+    assert "fp32 precision" in bench.metric_name(c3, "fp32")
+    assert bench.l2_note(c3, "mixed").startswith("inputs larger than L2")
+    c1.nz = 64  # 16 MiB of volume state: smaller than L2
+    assert bench.l2_note(c1, "fp32").startswith("inputs smaller than L2")
