@@ -162,9 +162,13 @@ class Pipeline:
                                    p.nz, C.byref(sse), None))
         return sse.value / (p.nx * p.ny * p.nz)
 
-    def gradient(self, params_d, x_rows) -> None:
-        """After reconstruct() + mse(with_grad=True): parameter gradient into self.dparams."""
+    def gradient(self, params_d, x_rows, fov_only: bool = False) -> None:
+        """After reconstruct() + mse(with_grad=True): parameter gradient into self.dparams.
+        fov_only: the gradient of the MSE over the fully sampled field of view alone (the
+        residual outside fov_mask() is zeroed before the adjoint)."""
         p = self.p
+        if fov_only:
+            self.res.mul_(self.fov_mask())
         self.grad.zero_()
         check(lib().fdk_bp_adjoint(C.byref(self.g), self.res.data_ptr(), self.mats_d.data_ptr(), p.nProj,
                                    self.grad.data_ptr(), None))
@@ -174,9 +178,10 @@ class Pipeline:
 
 def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 1000, params=None, log=print,
           time_limit_s: float | None = None, on_epoch=None, schedule: str = "constant",
-          input_window: str | None = None, batch: int = 1) -> dict:
+          input_window: str | None = None, batch: int = 1, loss_region: str = "volume") -> dict:
     """Adam on volume MSE; the training scans are generated once.  batch: phantoms per Adam
-    step (their gradients averaged; 1 = one phantom per step).
+    step (their gradients averaged; 1 = one phantom per step).  loss_region: "volume" (the
+    whole cube) or "fov" (the fully sampled field of view, Pipeline.fov_mask).
     schedule: "constant" (lr throughout) or "cosine" (lr decayed to lr/100 over all steps).
     on_epoch(epoch, params, history), when given, runs after every epoch (checkpointing)."""
     import torch
@@ -206,7 +211,7 @@ def train(n_train: int = 2000, epochs: int = 20, lr: float = 1e-3, seed0: int = 
                 pl.truth_of(seed0 + int(i))
                 pl.reconstruct(w, xs[i])
                 tot += pl.mse(with_grad=True)
-                pl.gradient(w, xs[i])
+                pl.gradient(w, xs[i], fov_only=loss_region == "fov")
                 if batch > 1:
                     gsum += pl.dparams
             n_done += batch

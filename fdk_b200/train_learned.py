@@ -1,7 +1,8 @@
 """Train and evaluate the learned residual row filter on the C5 workload.
 
     python -m fdk_b200.train_learned [--n-train 2000] [--epochs 20] [--n-test 200]
-                                      [--time-limit S] [--out fdk_b200/weights/residual_c5.npz]
+                                      [--loss-region volume|fov] [--time-limit S]
+                                      [--out fdk_b200/weights/residual_c5.npz]
     python -m fdk_b200.train_learned --eval-only [--out weights.npz]   # held-out result only
 
 Writes the trained parameters (npz) and prints one JSON line with the held-out result: MSE of
@@ -33,6 +34,8 @@ def main():
     ap.add_argument("--schedule", default="cosine", choices=["constant", "cosine"])
     ap.add_argument("--input-window", default=None, help="ramp window of the network's input rows (default: hann)")
     ap.add_argument("--batch", type=int, default=1, help="phantoms per Adam step (gradients averaged)")
+    ap.add_argument("--loss-region", default="volume", choices=["volume", "fov"],
+                    help="voxels of the training loss: the whole cube or the fully sampled field of view")
     ap.add_argument("--eval-only", action="store_true", help="evaluate the weights at --out, no training")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights",
                                                   "residual_c5.npz"))
@@ -54,11 +57,13 @@ def main():
                  input_window=window)
 
     tr = learned.train(args.n_train, args.epochs, args.lr, log=log, time_limit_s=args.time_limit, on_epoch=checkpoint,
-                       schedule=args.schedule, input_window=args.input_window, batch=args.batch)
+                       schedule=args.schedule, input_window=args.input_window, batch=args.batch,
+                       loss_region=args.loss_region)
     np.savez(args.out, params=tr["params"], history=np.asarray(tr["history"]), steps=tr["steps"], input_window=window)
     ev = learned.evaluate(tr["params"], args.n_test, input_window=args.input_window)
     out = {"workload": "C5: 256^3, 90 views of 256^2, I0=1e4, mu=0.02/mm", "n_train": args.n_train,
            "schedule": args.schedule, "input_window": window, "lr": args.lr, "batch": args.batch,
+           "loss_region": args.loss_region,
            "epochs_requested": args.epochs, "epochs_run": len(tr["history"]), "steps": tr["steps"],
            "stopped_early": tr["stopped_early"], "train_seconds": tr["seconds"], "history": tr["history"],
            "eval": ev, "total_seconds": time.time() - t0, "weights": os.path.relpath(args.out)}
