@@ -691,16 +691,20 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         except Exception:
             hbm_peak, hbm_src = 6650.0, "fallback"
         bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / max(1, len(batch_sizes))
-        traffic = read_traffic(f"bp_tma_{args.precision}_c2.md", f"dram_bytes_per_{BATCH}_view_batch_full")
+        # the staged kernel's DRAM bytes recorded by an ncu capture (MIXED: the interpolation layout)
+        traffic = read_traffic("bp_tma_lerp_c2.md" if args.precision == "mixed" else f"bp_tma_{args.precision}_c2.md",
+                               f"dram_bytes_per_{BATCH}_view_batch_full")
         if traffic is not None and bp_kind != "staged":
             traffic = None  # the figure is the staged kernel's
         nvox = param.nx * param.ny * param.nz
         if traffic is not None and nvox != 2048 ** 3:
             traffic *= nvox / 2048 ** 3  # recorded for 2048^3 (scaled by voxel count from a 512^3 capture)
         et = '__half2' if args.precision == 'mixed' else 'float2'
+        staged = ("bp_tma_kernel<HalfLerp> (views converted to the interpolation layout)" if args.precision == "mixed"
+                  else f"bp_tma_kernel<{et}>")
         roofline = {
             "kernel": {"quarter-turn": f"bp_sym_kernel<{et}> (views paired with their quarter-turn partners)",
-                       "staged": f"bp_tma_kernel<{et}>", "exact": "bp_exact_kernel"}[bp_kind],
+                       "staged": staged, "exact": "bp_exact_kernel"}[bp_kind],
             "bound": "smem" if peak_smem <= peak_fma else "fp32",
             "achieved": kernel_gups, "peak": peak, "unit": "GUPS", "frac": kernel_gups / peak,
             "traffic": traffic,

@@ -137,6 +137,26 @@ __global__ void transpose_views_kernel(const float *__restrict__ src, float *__r
 
 // Gather listed voxels (x, y, z of the whole volume) from the slab-pair volume [x][y][zs];
 // voxels outside the handle's boxes read NaN.  MIXED folds its compensation term.
+// MIRROR FP16 views -> the interpolation layout (HalfLerp): d = E(v+1) - E(v) rounded to FP16,
+// a = E(v) - d rounded, so a + d reproduces E(v) to one FP16 rounding; d = 0 at v = nv-1.
+__global__ void to_lerp_kernel(const __half2 *__restrict__ src, HalfLerp *__restrict__ dst, long long rows,
+                               int nv) {
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const __half2 *s = src + r * nv;
+        HalfLerp *d = dst + r * nv;
+        for (int v = threadIdx.x; v < nv; v += blockDim.x) {
+            const float2 e0 = __half22float2(s[v]);
+            const float2 e1 = v + 1 < nv ? __half22float2(s[v + 1]) : e0;
+            const __half2 dh = __floats2half2_rn(e1.x - e0.x, e1.y - e0.y);
+            const float2 df = __half22float2(dh);
+            HalfLerp o;
+            o.a = __floats2half2_rn(e0.x - df.x, e0.y - df.y);
+            o.d = dh;
+            d[v] = o;
+        }
+    }
+}
+
 __global__ void sample_voxels_kernel(const float *__restrict__ vol, const float *__restrict__ comp,
                                      const int *__restrict__ xyz, long long n, float *__restrict__ out, int x0,
                                      int y0, int nxs, int nys, long long tz0, long long td, long long bz0,
@@ -161,11 +181,11 @@ __global__ void sample_voxels_kernel(const float *__restrict__ vol, const float 
 using namespace fdk;
 
 namespace {
-// Most z bands per batch (tuning macro).  On the 2048^3 workload 8 bands measured the same as 4
-// (e2e 2203 against 2205 GUPS on one box): the readback then trails the PCIe copy, not the
-// first band.
+// Most z bands per batch (tuning macro).  On the 2048^3 workload 8 bands against 4: the same
+// device time (2383 against 2386 GUPS) and e2e 2182 against 2117 GUPS, as the readback of the
+// last band, which no backprojection hides, halves.
 #ifndef FDK_MAX_BANDS
-#define FDK_MAX_BANDS 4
+#define FDK_MAX_BANDS 8
 #endif
 constexpr int kMaxBands = FDK_MAX_BANDS;
 }
@@ -214,6 +234,13 @@ struct fdk_bp {
         ViewList views;
     };
     static constexpr int kListRing = 64;
+    // MIXED views of the list launches converted to the interpolation layout (HalfLerp), one
+    // buffer per source views buffer (the held and the filling batch of a reconstructor), tagged
+    // with the source; reserved by fdk_bp_reserve_lerp_internal
+    HalfLerp *d_lerp[2] = {nullptr, nullptr};
+    const void *lerp_src[2] = {nullptr, nullptr};
+    long long lerp_slots = 0;
+    int lerp_next = 0;
     ListRec *h_list = nullptr, *d_list = nullptr;
     cudaEvent_t list_ev[kListRing] = {};
     bool list_used[kListRing] = {};
@@ -581,6 +608,13 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             if (h->plan.tma_ok) {
                 s = precision == FDK_BP_MIXED ? tma_prepare<__half2>(h->plan.tma_ctas, device)
                                               : tma_prepare<float2>(h->plan.tma_ctas, device);
+                if (s == FDK_OK && precision == FDK_BP_MIXED) {
+                    int c = 0;
+                    s = tma_prepare<HalfLerp>(c, device);
+                    if (s == FDK_OK && c != h->plan.tma_ctas)
+                        s = fail(FDK_ERR_UNSUPPORTED, "interpolation-layout kernel: %d CTAs against %d", c,
+                                 h->plan.tma_ctas);
+                }
                 if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
                 if (s == FDK_OK) ck(cudaMemsetAsync(h->plan.d_err, 0, sizeof(unsigned int), h->stream), "error word");
                 if (s == FDK_OK)
@@ -610,7 +644,7 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         const void *kernels[] = {(const void *)transform_volume_kernel<true>,
                                  (const void *)transform_volume_kernel<false>, (const void *)absmax_kernel,
                                  (const void *)to_mirror_half_kernel, (const void *)to_mirror_kernel<float2>,
-                                 (const void *)fold_comp_kernel};
+                                 (const void *)fold_comp_kernel, (const void *)to_lerp_kernel};
         for (const void *kf : kernels)
             if (s == FDK_OK) ck(cudaFuncGetAttributes(&fa, kf), "kernel load");
     }
@@ -848,6 +882,8 @@ int fdk_bp_destroy(fdk_bp *h) {
                 cudaEventDestroy(h->list_ev[i]);
             }
         if (h->h_list) cudaFreeHost(h->h_list);
+        for (int i = 0; i < 2; i++)
+            if (h->d_lerp[i]) cudaFree(h->d_lerp[i]);
         if (h->d_list) cudaFree(h->d_list);
         for (int i = 0; i < 3; i++)
             if (h->sync_ev[i]) cudaEventDestroy(h->sync_ev[i]);
@@ -863,6 +899,30 @@ int fdk_bp_destroy(fdk_bp *h) {
 
 // Kernel launches of the handle since creation or the last reset (internal: recon.cu).
 long long fdk_bp_launches_internal(const fdk_bp *h) { return h ? h->launches : 0; }
+
+// Two interpolation-layout buffers of n_slots MIXED views each for fdk_bp_bp_lists_internal
+// (the held and the filling batch), allocated once, before the first launch.  Internal to the
+// library (recon.cu).
+int fdk_bp_reserve_lerp_internal(fdk_bp *h, int n_slots) {
+    FDK_ABI_BEGIN
+    FDK_CHECK_ARG(h && n_slots > 0, "NULL handle or no views");
+    if (h->precision != FDK_BP_MIXED || !h->plan.tma_ok || h->lerp_slots >= n_slots) return FDK_OK;
+    DeviceGuard dg(h->device);
+    FDK_TRY(dg.status);
+    FDK_TRY(collect_timers(h));  // no launch may still read the old buffers
+    const long long frame = (long long)h->plan.nu * h->plan.nv;
+    for (int i = 0; i < 2; i++) {
+        if (h->d_lerp[i]) cudaFree(h->d_lerp[i]);
+        h->d_lerp[i] = nullptr;
+        h->lerp_src[i] = nullptr;
+    }
+    h->lerp_slots = 0;
+    for (int i = 0; i < 2; i++)
+        FDK_CUDA(cudaMalloc(&h->d_lerp[i], sizeof(HalfLerp) * frame * n_slots));
+    h->lerp_slots = n_slots;
+    return FDK_OK;
+    FDK_ABI_END
+}
 
 // Device scalar multiplying the MIXED accumulators of device-resident FP16 views (their
 // producer divided the filtered values by it).  Internal to the library (recon.cu).
@@ -953,6 +1013,28 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
 }
 
 namespace {
+// The interpolation-layout copy of slots 0..n_slots-1 of a MIXED views buffer: converted on st
+// when the first (or only) band of a batch is launched (band <= 0), reused by its later bands.
+int lerp_views(fdk_bp *h, const void *views, int n_slots, int band, cudaStream_t st, HalfLerp **out) {
+    FDK_CHECK_ARG(h->lerp_slots >= n_slots, "interpolation-layout buffers of %lld views for a batch of %d",
+                  h->lerp_slots, n_slots);
+    int j = h->lerp_src[0] == views ? 0 : h->lerp_src[1] == views ? 1 : -1;
+    if (j < 0 || band <= 0) {
+        if (j < 0) {
+            j = h->lerp_next;
+            h->lerp_next ^= 1;
+        }
+        const long long rows = (long long)n_slots * h->plan.nu;
+        to_lerp_kernel<<<(int)std::min<long long>(rows, 148 * 16), 256, 0, st>>>(
+            static_cast<const __half2 *>(views), h->d_lerp[j], rows, h->plan.nv);
+        FDK_CUDA(cudaGetLastError());
+        h->launches++;
+        h->lerp_src[j] = views;
+    }
+    *out = h->d_lerp[j];
+    return FDK_OK;
+}
+
 // The next entry of the handle's list ring, once the launch that last read it has finished (a
 // bounded wait; immediate unless the host runs kListRing launches ahead of the device).
 int take_list(fdk_bp *h, fdk_bp::ListRec **rec, fdk_bp::ListRec **dev, int *entry) {
@@ -1000,6 +1082,13 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
     std::pair<cudaEvent_t, cudaEvent_t> tm;
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
+    HalfLerp *lv = nullptr;
+    if (mixed && n_single > 0) {
+        int used = 0;  // slots the singles read (a partial batch converts only its own)
+        for (int i = 0; i < n_single; i++) used = std::max(used, s_slot[i] + 1);
+        FDK_CHECK_ARG(used <= n_slots, "slot outside the views buffer");
+        FDK_TRY(lerp_views(h, views, used, band, st, &lv));
+    }
     for (int k = kb; k < ke; k++) {
         for (int q0 = 0; q0 < n_quad; q0 += kSymMaxQuads) {
             const int nq = std::min(kSymMaxQuads, n_quad - q0);
@@ -1031,13 +1120,16 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
             if (run) {
                 // consecutive views in consecutive slots: a launch without a list, over the
                 // buffer from the run's first slot (the kernel's loop then reads no list)
-                const size_t frame = (size_t)h->plan.nu * h->plan.nv * (mixed ? sizeof(__half2) : sizeof(float2));
-                const void *pv = static_cast<const char *>(views) + frame * s_slot[s0];
+                const size_t esz = lv ? sizeof(HalfLerp) : mixed ? sizeof(__half2) : sizeof(float2);
+                const size_t frame = (size_t)h->plan.nu * h->plan.nv * esz;
+                const void *pv = static_cast<const char *>(lv ? (const void *)lv : views) + frame * s_slot[s0];
                 const long long m0 = 12 * (long long)s_view[s0];
-                FDK_TRY(mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
-                                                       ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
-                              : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
-                                                      ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                FDK_TRY(lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                                                     ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
+                        : mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                                                         ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
+                                : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                                                        ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
                 h->launches++;
                 continue;
             }
@@ -1051,7 +1143,10 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 vl.view[i] = s_view[s0 + i];
             }
             FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(ViewList), cudaMemcpyHostToDevice, st));
-            const int r = mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
+            const int r = lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns, st,
+                                                       acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
+                                                       n_slots)
+                          : mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
                                                          acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
                                                          n_slots)
                                 : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,

@@ -81,6 +81,27 @@ struct TmaCfg<float2> {
     static constexpr int S = FDK_TMA_FP32_S;
 };
 
+// MIXED views in the interpolation layout: element (u, v) holds a = E(v) - d and d = E(v+1) -
+// E(v), E(v) the FP16 mirror pair of the MIRROR layout (d = 0 at v = nv-1, which no sample
+// reads).  A sample at v = vi + fv is then a + (1 + fv) d: one HFMA2 with the 1 + fv that the
+// fixed-point slice index yields, and one 8-byte load per detector column.
+struct __align__(8) HalfLerp {
+    __half2 a, d;
+};
+// Measured on the 2048^3 / 4096-view workload, 512-view batches, conversion included: 2644
+// against 2339 GUPS for the FP16 gather on one box (5 views per stage: slower).  The tile height
+// is the FP16 kernel's, so both cut the slab into the same z tiles and bands.
+#ifndef FDK_TMA_LERP_NV
+#define FDK_TMA_LERP_NV 4
+#endif
+template <>
+struct TmaCfg<HalfLerp> {
+    static constexpr int R = TmaCfg<__half2>::R;
+    static constexpr int BW = 34;  // 272 B rows: 68 words, an 8-row bank period for 8-byte loads
+    static constexpr int BH = 40;
+    static constexpr int NV = FDK_TMA_LERP_NV;
+    static constexpr int S = 2;
+};
 
 struct __align__(16) TmaMeta {
     float m[12];
@@ -137,6 +158,11 @@ __device__ __forceinline__ unsigned lds32(unsigned addr) {
 __device__ __forceinline__ float2 lds64f(unsigned addr) {
     float2 v;
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint2 lds64u(unsigned addr) {
+    uint2 v;
+    asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ __half2 u2h(unsigned u) { return *reinterpret_cast<__half2 *>(&u); }
@@ -250,7 +276,64 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
     const float fu = U - fuf;
     const int u0 = (int)fuf;
 
-    if constexpr (!std::is_same<E, float2>::value) {
+    if constexpr (std::is_same<E, HalfLerp>::value) {
+        constexpr unsigned RB = C::BW * 8;  // box row bytes
+        const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
+        if (md.staged) {
+            // fixed point as in the FP16 gather: bits = 0x4B400000 + round(1024 (v - v_lo))
+            const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
+            const float B1 = B * 1024.f;
+            const unsigned rowp = box + (unsigned)(u0 - md.u_lo) * RB - (0x4B400000u >> 10) * 8u;
+            if (md.interior) {
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+                    const unsigned a = rowp + (bits >> 10) * 8u;
+                    const __half2 g = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
+                    const uint2 p0 = lds64u(a), p1 = lds64u(a + RB);
+                    const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
+                    const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
+                    acc_add_f16x2(am[k], ar[k], __hfma2(l1, bw, __hmul2(l0, aw)));
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < R; k++) {
+                    const float v = fmaf(B, (float)k, A);
+                    const float vr = (float)(nv - 1) - v;
+                    const bool mv = v >= 0.f && v < (float)(nv - 1);
+                    const bool rv = vr >= 0.f && vr < (float)(nv - 1);
+                    if (!(mv || rv)) continue;
+                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+                    const unsigned a = rowp + (bits >> 10) * 8u;
+                    const __half2 g = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));
+                    const uint2 p0 = lds64u(a), p1 = lds64u(a + RB);
+                    const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
+                    const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
+                    const float2 rf = __half22float2(__hfma2(l1, bw, __hmul2(l0, aw)));
+                    if (mv) am[k] += rf.x;
+                    if (rv) ar[k] += rf.y;
+                }
+            }
+            return;
+        }
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+            const float v = fmaf(B, (float)k, A);
+            const float vr = (float)(nv - 1) - v;
+            const bool mv = v >= 0.f && v < (float)(nv - 1);
+            const bool rv = vr >= 0.f && vr < (float)(nv - 1);
+            if (!(mv || rv)) continue;
+            const float vf = fminf(floorf(v), (float)(nv - 2));
+            const __half2 g = __float2half2_rn(1.0f + (v - vf));
+            const uint2 *g0 = reinterpret_cast<const uint2 *>(gview) + (long long)u0 * nv + (int)vf;
+            const uint2 p0 = __ldg(g0), p1 = __ldg(g0 + nv);
+            const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
+            const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
+            const float2 rf = __half22float2(__hfma2(l1, bw, __hmul2(l0, aw)));
+            if (mv) am[k] += rf.x;
+            if (rv) ar[k] += rf.y;
+        }
+    } else if constexpr (!std::is_same<E, float2>::value) {
         using G = HalfGather<E>;
         constexpr unsigned RB = C::BW * G::ESZ;  // box row bytes
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);

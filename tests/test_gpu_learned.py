@@ -172,3 +172,18 @@ def test_trained_weights_beat_plain_fdk_on_held_out_scans():
     print(ev)
     assert ev["learned_better_frac"] == 1.0
     assert ev["mse_reduction"] >= 0.10, ev
+
+
+def test_field_of_view_weights_beat_plain_fdk_inside_the_field_of_view():
+    """The C5 network trained on the loss over the fully sampled field of view
+    (fdk_b200/weights/residual_c5_fov.npz, `train_learned --loss-region fov`) against plain FDK
+    on held-out phantoms: lower MSE on every scan, and inside the field of view a larger cut than
+    the volume-trained weights give there (the 200-scan figures are in residual_c5_fov.json)."""
+    import os
+
+    path = os.path.join(os.path.dirname(Lr.__file__), "weights", "residual_c5_fov.npz")
+    d = np.load(path)
+    ev = Lr.evaluate(d["params"], n_test=8, seed0=5000)
+    print(ev)
+    assert ev["learned_better_frac"] == 1.0
+    assert ev["fov_mse_reduction"] >= 0.17, ev

@@ -238,7 +238,8 @@ def test_z_bands_and_overlapped_readback(precision, monkeypatch):
     mid, _ = run(True)
     monkeypatch.setenv("FDK_BP_BANDS", "1")
     single, l_single = run(False)
-    assert l_banded - l_single == 2 * 3  # two batches of 16 views, 4 bands instead of 1
+    # two batches of 16 views, each as several band launches instead of one
+    assert l_banded > l_single and (l_banded - l_single) % 2 == 0
     assert np.array_equal(banded, single)
     assert np.array_equal(mid, banded)
     assert np.abs(banded).max() > 0
