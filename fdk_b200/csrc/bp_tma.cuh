@@ -94,13 +94,22 @@ struct __align__(8) HalfLerp {
 #ifndef FDK_TMA_LERP_NV
 #define FDK_TMA_LERP_NV 4
 #endif
+#ifndef FDK_TMA_LERP_BW
+#define FDK_TMA_LERP_BW 34
+#endif
+#ifndef FDK_TMA_LERP_BH
+#define FDK_TMA_LERP_BH 40
+#endif
+#ifndef FDK_TMA_LERP_S
+#define FDK_TMA_LERP_S 2
+#endif
 template <>
 struct TmaCfg<HalfLerp> {
     static constexpr int R = TmaCfg<__half2>::R;
-    static constexpr int BW = 34;  // 272 B rows: 68 words, an 8-row bank period for 8-byte loads
-    static constexpr int BH = 40;
+    static constexpr int BW = FDK_TMA_LERP_BW;  // 34: 272 B rows, 68 words, an 8-row bank period for 8-byte loads
+    static constexpr int BH = FDK_TMA_LERP_BH;
     static constexpr int NV = FDK_TMA_LERP_NV;
-    static constexpr int S = 2;
+    static constexpr int S = FDK_TMA_LERP_S;
 };
 
 struct __align__(16) TmaMeta {
@@ -316,6 +325,10 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
             }
             return;
         }
+        // a tile whose footprint does not fit the box: the column's two detector rows from global
+        // memory (row pointer formed once; rare, and kept lean so the hot loops above keep their
+        // registers)
+        const uint2 *grow = reinterpret_cast<const uint2 *>(gview) + (long long)u0 * nv;
 #pragma unroll
         for (int k = 0; k < R; k++) {
             const float v = fmaf(B, (float)k, A);
@@ -325,8 +338,8 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
             if (!(mv || rv)) continue;
             const float vf = fminf(floorf(v), (float)(nv - 2));
             const __half2 g = __float2half2_rn(1.0f + (v - vf));
-            const uint2 *g0 = reinterpret_cast<const uint2 *>(gview) + (long long)u0 * nv + (int)vf;
-            const uint2 p0 = __ldg(g0), p1 = __ldg(g0 + nv);
+            const int vi = (int)vf;
+            const uint2 p0 = __ldg(grow + vi), p1 = __ldg(grow + nv + vi);
             const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
             const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
             const float2 rf = __half22float2(__hfma2(l1, bw, __hmul2(l0, aw)));
