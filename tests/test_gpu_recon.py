@@ -338,3 +338,26 @@ def test_mixed_interpolation_layout_at_detector_edges():
     print("mixed vs fp64", e64, "vs fp32", e32, "masked voxels", int((~m).sum()))
     assert np.abs(vols["mixed"]).max() > 0
     assert e64 <= 1e-3 and e32 <= 1e-3
+
+
+def test_mixed_tiles_that_miss_their_box_read_global_memory():
+    """A detector four times finer than the voxel grid: every tile's footprint is wider than the
+    staged kernel's shared-memory box, so the MIXED reconstructor's interpolation-layout kernel
+    gathers every sample from global memory.  Against the FP64 pipeline and FP32."""
+    n, views = 32, 16
+    p = small_param(n, 128, 128, views)
+    _, proj = phantom_views(p, seed=12)
+    vols = {}
+    for prec in ("mixed", "fp32"):
+        r = F.Reconstructor(p, prec, batch=16)
+        r.push(proj.copy(), 0)
+        vols[prec] = r.volume().astype(np.float64)
+        r.close()
+    top = [0, 0, 0, n, n, n // 2]
+    filt = oracle_filtered(p, proj, pad_n=4)
+    f64, _ = oracle_bp_f64(top, n // 2, n, filt, p.proj_matrices(np.float64))
+    m = knife_edge_mask(p, top, n // 2)
+    e64 = rel_l2(vols["mixed"][m], f64[m])
+    e32 = rel_l2(vols["fp32"][m], f64[m])
+    print("mixed vs fp64", e64, "fp32 vs fp64", e32)
+    assert e64 <= 1e-3 and e32 <= 1e-5

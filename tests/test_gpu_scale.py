@@ -151,6 +151,32 @@ def test_c2_full_size_all_precisions():
     _full_size_check("c2", 2, 20, cpu_slab=64)
 
 
+def test_c4_full_size_mixed_and_fp32_vs_fp64():
+    """C4 (1024^3 from 1024 views of 1536 x 1024): 1.5 detector pixels per voxel, so about 1% of
+    the staged kernels' (tile, view) footprints exceed their shared-memory box and are gathered
+    from global memory.  MIXED and FP32 against the FP64 oracle at 1e5 seeded voxels and the
+    central slices."""
+    p = F.config("c4")
+    n = p.nx
+    dev = _views(p, 4, 30)
+    host = dev.cpu().numpy()
+    vox = O.sample_voxels(n, n, n, 100000, 4)
+    got = {}
+    for prec in ("fp32", "mixed"):
+        r = _recon(p, prec, dev)
+        got[prec] = r.sample(vox)
+        r.close()
+    del dev
+    S4 = O.SampledFDK(p, vox, pad_n=4)
+    for c in range(0, p.nProj, 64):
+        S4.add(host[c:c + 64], c)
+    edge = S4.edge.astype(bool)
+    errs = {prec: _err(got[prec], S4.values, edge) for prec in got}
+    print("c4", errs)
+    assert errs["mixed"]["all"] <= 1e-3 and errs["mixed"]["masked"] <= 1e-3
+    assert errs["fp32"]["masked"] <= 1e-5
+
+
 def test_c2_slab_pair_mixed_vs_fp64_and_fp32_vs_reference_arithmetic():
     """A central 2 x 64-slice slab pair of the 512^3 volume (one rank's share)."""
     p = F.config("c2")
