@@ -995,13 +995,14 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
         }
     if (!r) return FDK_OK;
     const bool mixed = h->precision == FDK_BP_MIXED;
-    const int R = mixed ? SymCfg<__half2>::R : SymCfg<float2>::R;
-    const int BW = mixed ? SymCfg<__half2>::BW : SymCfg<float2>::BW;
-    const int BH = mixed ? SymCfg<__half2>::BH : SymCfg<float2>::BH;
+    // MIXED pairs views over the interpolation layout (8-byte elements)
+    const int R = mixed ? SymCfg<HalfLerp>::R : SymCfg<float2>::R;
+    const int BW = mixed ? SymCfg<HalfLerp>::BW : SymCfg<float2>::BW;
+    const int BH = mixed ? SymCfg<HalfLerp>::BH : SymCfg<float2>::BH;
     if (!sym_footprints_fit(mats, n_proj, h->nx, p.z0, p.nzz, R, BW, BH)) return FDK_OK;
     DeviceGuard dg(h->device);
     FDK_TRY(dg.status);
-    FDK_TRY(mixed ? sym_prepare<__half2>(h->sym_ctas, h->device) : sym_prepare<float2>(h->sym_ctas, h->device));
+    FDK_TRY(mixed ? sym_prepare<HalfLerp>(h->sym_ctas, h->device) : sym_prepare<float2>(h->sym_ctas, h->device));
     // bands on whole tiles of both kernels (set up before the first launch)
     const int Rt = mixed ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
     int unit = Rt;
@@ -1083,9 +1084,10 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
     HalfLerp *lv = nullptr;
-    if (mixed && n_single > 0) {
-        int used = 0;  // slots the singles read (a partial batch converts only its own)
+    if (mixed) {
+        int used = 0;  // slots the launches read (a partial batch converts only its own)
         for (int i = 0; i < n_single; i++) used = std::max(used, s_slot[i] + 1);
+        for (int i = 0; i < 4 * n_quad; i++) used = std::max(used, q_slot[i] + 1);
         FDK_CHECK_ARG(used <= n_slots, "slot outside the views buffer");
         FDK_TRY(lerp_views(h, views, used, band, st, &lv));
     }
@@ -1102,9 +1104,9 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 sq.view[i] = q_view[q0 + i];
             }
             FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(SymQuads), cudaMemcpyHostToDevice, st));
-            const int r = mixed ? bp_sym_launch<__half2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots,
-                                                         d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
-                                                         acc_scale, h->band_z[k], h->band_z[k + 1])
+            const int r = mixed ? bp_sym_launch<HalfLerp>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, lv, n_slots,
+                                                          d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
+                                                          acc_scale, h->band_z[k], h->band_z[k + 1])
                                 : bp_sym_launch<float2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots,
                                                         d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
                                                         acc_scale, h->band_z[k], h->band_z[k + 1]);

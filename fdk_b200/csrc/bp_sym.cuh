@@ -19,14 +19,11 @@
 //    tile (8 corners) and issues four 3-D TMA tile loads (no multicast) of that box, one from
 //    each member view's slot in the views buffer, into a ring of S stages completed by
 //    mbarrier expect_tx; consumers release a stage through a second mbarrier.
-//  * MIXED: v in fixed point as bp_tma.cuh (t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per
-//    slice gives the box index and the 10-bit fraction); the four bilinear weights are formed
-//    once per slice and shared by the four views.  FDK_SYM_INTERP selects the interpolation:
-//    0 (default) FP16 products summed by HFMA2 into one FP16 pair per view, added to the FP32
-//    accumulators by the sm_100 mixed-precision add; 1 the sm_100 mixed-precision FMA
-//    (fma.rn.f32.f16: FP16 texel x FP16 weight, exact product, FP32 sum) straight into the FP32
-//    accumulators.
-//  * FP32: the same with FP32 pairs and FFMA.
+//  * MIXED reads the views in the interpolation layout (HalfLerp, bp_tma.cuh): v in fixed point
+//    (t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per slice gives the box index and 1 + fv),
+//    and per member two 8-byte loads and a + (1 + fv) d per detector column, then the u-lerp;
+//    the FP16 pair is added to the FP32 accumulators by the sm_100 mixed-precision add.
+//  * FP32: FP32 mirror pairs, the four bilinear weights formed once per slice, FFMA.
 //  * The host admits a launch only when every tile's footprint fits the box in every base view
 //    (sym_footprints_fit); a quadruple whose box would not fit is skipped and reported through
 //    the device error word (kErrFootprint) rather than gathered from global memory, which would
@@ -46,18 +43,6 @@ namespace fdk {
 #ifndef FDK_SYM_MIXED_R
 #define FDK_SYM_MIXED_R 6
 #endif
-#ifndef FDK_SYM_MIXED_BW
-#define FDK_SYM_MIXED_BW 28
-#endif
-#ifndef FDK_SYM_MIXED_NQ
-#define FDK_SYM_MIXED_NQ 3
-#endif
-#ifndef FDK_SYM_MIXED_S
-#define FDK_SYM_MIXED_S 2
-#endif
-#ifndef FDK_SYM_MIXED_BH
-#define FDK_SYM_MIXED_BH 32
-#endif
 #ifndef FDK_SYM_FP32_R
 #define FDK_SYM_FP32_R 6
 #endif
@@ -73,36 +58,22 @@ namespace fdk {
 #ifndef FDK_SYM_FP32_S
 #define FDK_SYM_FP32_S 2
 #endif
-#ifndef FDK_SYM_INTERP
-#define FDK_SYM_INTERP 0
-#endif
 
 // Tile and pipeline shapes (macros for tuning sweeps), measured on one B200 (GUPS of the kernel,
 // 512-view batches in the bench's quarter read order; staged = bp_tma_kernel on the same views):
 //   FP32:  C2 1227 staged -> 1777 (R 6, 34 x 40 boxes, 1 quad x 2 stages) -> 1908 (18 x 32 boxes,
 //          2 quads x 3 stages); C3 1257 staged -> 1749.  R 4 at 64 registers (3 CTAs per SM):
 //          1895 at C2 but 1426 at C3 (short volume runs).
-//   MIXED: C2 2320 staged against 2090-2229 for every shape tried (R 4-6, 20-28 x 32-40 boxes,
-//          2-4 quads, 2-4 stages, 2 or 3 CTAs per SM, FP16 or mixed-FMA interpolation); C3 2358
-//          staged against 2084.  The FP16 kernel sits near 57% of its shared-memory wavefront
-//          bound (issue 39%, latency-bound at 4 consumer warps per scheduler and 96 registers)
-//          while the FP32 one saturates its bound; the reconstructor therefore pairs views for
-//          FP32 only unless FDK_BP_SYM=1.
+//   MIXED, FP16 mirror pairs (this kernel's first MIXED form, since removed): C2 2320 staged
+//          against 2090-2229 for every shape tried (R 4-6, 20-28 x 32-40 boxes, 2-4 quads, 2-4
+//          stages, 2 or 3 CTAs per SM, FP16 or mixed-FMA interpolation); C3 2358 staged against
+//          2084 -- near 57% of its shared-memory wavefront bound, issue 39%, latency-bound at 4
+//          consumer warps per scheduler and 96 registers.
+//   MIXED, interpolation layout (the FP32 shape): C2 2649 staged -> 2150, C3 2719 -> 1887.
+//   The reconstructor therefore pairs views for FP32 only unless FDK_BP_SYM=1.
 // At 112 registers (one CTA per SM: 9 warps) both ran at 1440-1630.
 template <typename E>
 struct SymCfg;
-template <>
-struct SymCfg<__half2> {
-    static constexpr int R = FDK_SYM_MIXED_R;    // top-slab slices per thread (registers: see below)
-    // box width (v elements; x 4 B a multiple of 16 B).  The row pitch sets the bank pattern of
-    // the 8 x 4 lane block, whose samples fall on about ten rows at nearly the same v: 20 or 28
-    // words repeat every 8 rows, 24 words every 4 (2-3x the shared wavefronts); 28 also leaves
-    // room for the volume's top and bottom tiles (footprint check).
-    static constexpr int BW = FDK_SYM_MIXED_BW;
-    static constexpr int BH = FDK_SYM_MIXED_BH;  // box height (u rows)
-    static constexpr int NQ = FDK_SYM_MIXED_NQ;  // quadruples per stage
-    static constexpr int S = FDK_SYM_MIXED_S;    // stages
-};
 template <>
 struct SymCfg<float2> {
     static constexpr int R = FDK_SYM_FP32_R;
@@ -111,6 +82,19 @@ struct SymCfg<float2> {
     static constexpr int BW = FDK_SYM_FP32_BW;
     static constexpr int BH = FDK_SYM_FP32_BH;
     static constexpr int NQ = FDK_SYM_FP32_NQ;
+    static constexpr int S = FDK_SYM_FP32_S;
+};
+// MIXED views in the interpolation layout (HalfLerp, 8-byte elements): the FP32 kernel's box and
+// stage shape (the same element size); R = 6 keeps the 4 x 2 x R accumulators in 96 registers.
+#ifndef FDK_SYM_LERP_NQ
+#define FDK_SYM_LERP_NQ 2
+#endif
+template <>
+struct SymCfg<HalfLerp> {
+    static constexpr int R = FDK_SYM_MIXED_R;
+    static constexpr int BW = FDK_SYM_FP32_BW;
+    static constexpr int BH = FDK_SYM_FP32_BH;
+    static constexpr int NQ = FDK_SYM_LERP_NQ;
     static constexpr int S = FDK_SYM_FP32_S;
 };
 
@@ -196,23 +180,6 @@ __device__ __forceinline__ void sym_tile_box(const float *m, float xa, float xb,
     md.interior = (vmin > 1e-3f && vmax < (float)(nv - 1) - 1e-3f) ? 1 : 0;
 }
 
-__device__ __forceinline__ void mixed_fma4(float &acc_m, float &acc_r, __half2 e0, __half2 e1, __half2 e2,
-                                           __half2 e3, __half2 w01, __half2 w23) {
-    // acc_m += e0.lo w0 + e1.lo w1 + e2.lo w2 + e3.lo w3, acc_r the same on the high halves;
-    // w01 = (w0, w1), w23 = (w2, w3): FP16 x FP16 products are exact in FP32
-    asm("{\n .reg .f16 a0, b0, a1, b1, a2, b2, a3, b3, w0, w1, w2, w3;\n"
-        " mov.b32 {a0, b0}, %2;\n mov.b32 {a1, b1}, %3;\n mov.b32 {a2, b2}, %4;\n mov.b32 {a3, b3}, %5;\n"
-        " mov.b32 {w0, w1}, %6;\n mov.b32 {w2, w3}, %7;\n"
-        " fma.rn.f32.f16 %0, a0, w0, %0;\n fma.rn.f32.f16 %1, b0, w0, %1;\n"
-        " fma.rn.f32.f16 %0, a1, w1, %0;\n fma.rn.f32.f16 %1, b1, w1, %1;\n"
-        " fma.rn.f32.f16 %0, a2, w2, %0;\n fma.rn.f32.f16 %1, b2, w2, %1;\n"
-        " fma.rn.f32.f16 %0, a3, w3, %0;\n fma.rn.f32.f16 %1, b3, w3, %1;\n}"
-        : "+f"(acc_m), "+f"(acc_r)
-        : "r"(*reinterpret_cast<unsigned *>(&e0)), "r"(*reinterpret_cast<unsigned *>(&e1)),
-          "r"(*reinterpret_cast<unsigned *>(&e2)), "r"(*reinterpret_cast<unsigned *>(&e3)),
-          "r"(*reinterpret_cast<unsigned *>(&w01)), "r"(*reinterpret_cast<unsigned *>(&w23)));
-}
-
 // One quadruple's contribution to a thread's four columns: 4 x R voxel pairs.  box: the four
 // member boxes (staged footprints), BOX bytes apart.
 template <typename E>
@@ -237,59 +204,41 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
     const float fu = U - fuf;
     const int u0 = (int)fuf;
 
-    if constexpr (!std::is_same<E, float2>::value) {
-        constexpr unsigned RB = C::BW * 4;  // box row bytes
+    if constexpr (std::is_same<E, HalfLerp>::value) {
+        // one address, fraction and u-weight set per slice serves the four members: per member
+        // two 8-byte loads (the sample's two detector columns) and a + (1 + fv) d per column
+        constexpr unsigned RB = C::BW * 8;
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
-        const __half2 one = __float2half2_rn(1.f);
-        {  // staged: the host checked that every tile's footprint fits the box (sym_footprints_fit)
-            const float C0 = fmaf(A - (float)v_lo, 1024.f, 12582912.f);
-            const float B1 = B * 1024.f;
-            const unsigned rowp = box + (unsigned)(u0 - u_lo) * RB - (0x4B400000u >> 10) * 4u;
+        const float C0 = fmaf(A - (float)v_lo, 1024.f, 12582912.f);
+        const float B1 = B * 1024.f;
+        const unsigned rowp = box + (unsigned)(u0 - u_lo) * RB - (0x4B400000u >> 10) * 8u;
 #pragma unroll
-            for (int k = 0; k < R; k++) {
-                bool mv = true, rv = true;
-                if (!interior) {
-                    // slices near the detector's top or bottom edge: SUBPIXEL's bounds per slice
-                    const float v = fmaf(B, (float)k, A);
-                    const float vr = (float)(nv - 1) - v;
-                    mv = v >= 0.f && v < (float)(nv - 1);
-                    rv = vr >= 0.f && vr < (float)(nv - 1);
-                    if (!(mv || rv)) continue;
-                }
-                const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
-                const unsigned a = rowp + (bits >> 10) * 4u;
-                const __half2 fv = __hsub2(__low2half2(u2h((bits & 0x3FFu) | 0x3C00u)), one);  // exact
-                const __half2 w1 = __hmul2(aw, fv), w3 = __hmul2(bw, fv);
-                const __half2 w0 = __hsub2(aw, w1), w2 = __hsub2(bw, w3);
-#if FDK_SYM_INTERP == 1
-                const __half2 w01 = __lows2half2(w0, w1), w23 = __lows2half2(w2, w3);
-#endif
+        for (int k = 0; k < R; k++) {
+            bool mv = true, rv = true;
+            if (!interior) {
+                const float v = fmaf(B, (float)k, A);
+                const float vr = (float)(nv - 1) - v;
+                mv = v >= 0.f && v < (float)(nv - 1);
+                rv = vr >= 0.f && vr < (float)(nv - 1);
+                if (!(mv || rv)) continue;
+            }
+            const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
+            const unsigned a = rowp + (bits >> 10) * 8u;
+            const __half2 g = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const __half2 e0 = u2h(lds32(a + j * BOX)), e1 = u2h(lds32(a + j * BOX + 4));
-                    const __half2 e2 = u2h(lds32(a + j * BOX + RB)), e3 = u2h(lds32(a + j * BOX + RB + 4));
-#if FDK_SYM_INTERP == 1
-                    if (interior) {
-                        mixed_fma4(am[j][k], ar[j][k], e0, e1, e2, e3, w01, w23);
-                    } else {
-                        float tm = 0.f, tr = 0.f;
-                        mixed_fma4(tm, tr, e0, e1, e2, e3, w01, w23);
-                        if (mv) am[j][k] += tm;
-                        if (rv) ar[j][k] += tr;
-                    }
-#else
-                    const __half2 r = __hfma2(e3, w3, __hfma2(e2, w2, __hfma2(e1, w1, __hmul2(e0, w0))));
-                    if (interior) {
-                        acc_add_f16x2(am[j][k], ar[j][k], r);
-                    } else {
-                        const float2 rf = __half22float2(r);
-                        if (mv) am[j][k] += rf.x;
-                        if (rv) ar[j][k] += rf.y;
-                    }
-#endif
+            for (int j = 0; j < 4; j++) {
+                const uint2 p0 = lds64u(a + j * BOX), p1 = lds64u(a + j * BOX + RB);
+                const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
+                const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
+                const __half2 r = __hfma2(l1, bw, __hmul2(l0, aw));
+                if (interior) {
+                    acc_add_f16x2(am[j][k], ar[j][k], r);
+                } else {
+                    const float2 rf = __half22float2(r);
+                    if (mv) am[j][k] += rf.x;
+                    if (rv) ar[j][k] += rf.y;
                 }
             }
-            return;
         }
     } else {
         const float wa = (1.f - fu) * wt, wb = fu * wt;
