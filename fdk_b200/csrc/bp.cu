@@ -241,6 +241,13 @@ struct fdk_bp {
     const void *lerp_src[2] = {nullptr, nullptr};
     long long lerp_slots = 0;
     int lerp_next = 0;
+    // MIXED views of the BackProjectionFDK calls (fdk_bp_bp, fdk_bp_bp_device) in the
+    // interpolation layout: allocated at the first call, reused once the event recorded after
+    // the last call's launches has passed on the next call's stream
+    HalfLerp *d_lerp_call = nullptr;
+    long long lerp_call_cap = 0;
+    cudaEvent_t lerp_call_ev = nullptr;
+    bool lerp_call_used = false;
     ListRec *h_list = nullptr, *d_list = nullptr;
     cudaEvent_t list_ev[kListRing] = {};
     bool list_used[kListRing] = {};
@@ -280,6 +287,29 @@ int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
 //   layout MIRROR: mirror pairs (f32x2 or f16x2 per precision), proj_h rows x proj_w pairs
 //   band: -1 = every z band (the whole volume), else that band only (views counted with band 0;
 //   kernels without bands run whole with band 0 and do nothing for the others)
+// The n MIRROR FP16 views of a BackProjectionFDK call converted to the interpolation layout on
+// st (after the previous call's launches, which may have read the buffer on another stream).
+int lerp_call_views(fdk_bp *h, const void *dev_proj, int n, cudaStream_t st, HalfLerp **out) {
+    const long long frame = (long long)h->plan.nu * h->plan.nv;
+    if (!h->lerp_call_ev) FDK_CUDA(cudaEventCreateWithFlags(&h->lerp_call_ev, cudaEventDisableTiming));
+    if (h->lerp_call_cap < n) {
+        if (h->lerp_call_used) FDK_TRY(wait_event(h->lerp_call_ev, "view conversion"));
+        if (h->d_lerp_call) cudaFree(h->d_lerp_call);
+        h->d_lerp_call = nullptr;
+        h->lerp_call_cap = 0;
+        FDK_CUDA(cudaMalloc(&h->d_lerp_call, sizeof(HalfLerp) * frame * n));
+        h->lerp_call_cap = n;
+    }
+    if (h->lerp_call_used) FDK_CUDA(cudaStreamWaitEvent(st, h->lerp_call_ev, 0));
+    const long long rows = (long long)n * h->plan.nu;
+    to_lerp_kernel<<<(int)std::min<long long>(rows, 148 * 16), 256, 0, st>>>(static_cast<const __half2 *>(dev_proj),
+                                                                           h->d_lerp_call, rows, h->plan.nv);
+    FDK_CUDA(cudaGetLastError());
+    h->launches++;
+    *out = h->d_lerp_call;
+    return FDK_OK;
+}
+
 int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const float *d_mats,
               const float *host_mats, int n, int width, int height, cudaStream_t st,
               const float *acc_scale = nullptr, int band = -1) {
@@ -319,15 +349,22 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
     } else {
         FDK_CHECK_ARG(layout == FDK_LAYOUT_MIRROR, "fast backprojection reads the MIRROR layout");
         if (h->plan.tma_ok && ((uintptr_t)dev_proj & 15) == 0) {
+            // MIXED: the views once in the interpolation layout, read by every band's launch
+            HalfLerp *lv = nullptr;
+            if (h->precision == FDK_BP_MIXED) FDK_TRY(lerp_call_views(h, dev_proj, n, st, &lv));
             for (int k = kb; k < ke; k++) {
-                if (h->precision == FDK_BP_MIXED)
-                    FDK_TRY(bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
-                                                   acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                if (lv)
+                    FDK_TRY(bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, n, st,
+                                                    acc_scale, h->band_tz[k], h->band_tz[k + 1]));
                 else
                     FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
                                                   acc_scale, h->band_tz[k], h->band_tz[k + 1]));
                 h->launches++;
                 FDK_CUDA(cudaEventRecord(h->band_done[k], st));
+            }
+            if (lv) {
+                FDK_CUDA(cudaEventRecord(h->lerp_call_ev, st));
+                h->lerp_call_used = true;
             }
         } else {
             const float ws = weight_scale(host_mats, h->top.x + 0.5f * (h->top.width - 1),
@@ -417,7 +454,7 @@ int read_volume(fdk_bp *h, float *host) {
 // common multiple of it and the quarter-turn kernel's once that kernel is set up; each boundary
 // is the whole unit nearest an even split of the slices.
 void set_bands(fdk_bp *h, int unit) {
-    const int R = h->precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+    const int R = h->precision == FDK_BP_MIXED ? TmaCfg<HalfLerp>::R : TmaCfg<float2>::R;
     const long long depth = (long long)h->top.depth;
     const long long cols = ceil_div((long long)h->top.width, 16) * ceil_div((long long)h->top.height, 16);
     const int tiles_z = (int)ceil_div(depth, R);
@@ -606,15 +643,8 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             const char *sel = getenv("FDK_BP_KERNEL");
             h->plan.tma_ok = ((size_t)proj_width * esz) % 16 == 0 && !(sel && std::string(sel) == "staged");
             if (h->plan.tma_ok) {
-                s = precision == FDK_BP_MIXED ? tma_prepare<__half2>(h->plan.tma_ctas, device)
+                s = precision == FDK_BP_MIXED ? tma_prepare<HalfLerp>(h->plan.tma_ctas, device)
                                               : tma_prepare<float2>(h->plan.tma_ctas, device);
-                if (s == FDK_OK && precision == FDK_BP_MIXED) {
-                    int c = 0;
-                    s = tma_prepare<HalfLerp>(c, device);
-                    if (s == FDK_OK && c != h->plan.tma_ctas)
-                        s = fail(FDK_ERR_UNSUPPORTED, "interpolation-layout kernel: %d CTAs against %d", c,
-                                 h->plan.tma_ctas);
-                }
                 if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
                 if (s == FDK_OK) ck(cudaMemsetAsync(h->plan.d_err, 0, sizeof(unsigned int), h->stream), "error word");
                 if (s == FDK_OK)
@@ -629,7 +659,7 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
     h->band_z[0] = 0;
     h->band_z[1] = (long long)t.depth;
     if (s == FDK_OK && h->plan.tma_ok && sym)
-        set_bands(h, precision == FDK_BP_MIXED ? TmaCfg<__half2>::R : TmaCfg<float2>::R);
+        set_bands(h, precision == FDK_BP_MIXED ? TmaCfg<HalfLerp>::R : TmaCfg<float2>::R);
     for (int k = 0; k < kMaxBands && s == FDK_OK; k++)
         ck(cudaEventCreateWithFlags(&h->band_done[k], cudaEventDisableTiming), "event");
     for (int i = 0; i < 2 && s == FDK_OK; i++)
@@ -884,6 +914,11 @@ int fdk_bp_destroy(fdk_bp *h) {
         if (h->h_list) cudaFreeHost(h->h_list);
         for (int i = 0; i < 2; i++)
             if (h->d_lerp[i]) cudaFree(h->d_lerp[i]);
+        if (h->lerp_call_ev) {
+            if (h->lerp_call_used) wait_event(h->lerp_call_ev, "view conversion");
+            cudaEventDestroy(h->lerp_call_ev);
+        }
+        if (h->d_lerp_call) cudaFree(h->d_lerp_call);
         if (h->d_list) cudaFree(h->d_list);
         for (int i = 0; i < 3; i++)
             if (h->sync_ev[i]) cudaEventDestroy(h->sync_ev[i]);
@@ -1004,7 +1039,7 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
     FDK_TRY(dg.status);
     FDK_TRY(mixed ? sym_prepare<HalfLerp>(h->sym_ctas, h->device) : sym_prepare<float2>(h->sym_ctas, h->device));
     // bands on whole tiles of both kernels (set up before the first launch)
-    const int Rt = mixed ? TmaCfg<__half2>::R : TmaCfg<float2>::R;
+    const int Rt = mixed ? TmaCfg<HalfLerp>::R : TmaCfg<float2>::R;
     int unit = Rt;
     while (unit % R) unit += Rt;
     set_bands(h, unit);
@@ -1128,10 +1163,8 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 const long long m0 = 12 * (long long)s_view[s0];
                 FDK_TRY(lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
                                                      ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
-                        : mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
-                                                         ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
-                                : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
-                                                        ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                        : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0, ns,
+                                                st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
                 h->launches++;
                 continue;
             }
@@ -1148,12 +1181,8 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
             const int r = lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns, st,
                                                        acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
                                                        n_slots)
-                          : mixed ? bp_tma_launch<__half2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
-                                                         acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
-                                                         n_slots)
-                                : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
-                                                        acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
-                                                        n_slots);
+                          : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
+                                                  acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views, n_slots);
             FDK_TRY(release_list(h, e, st));
             FDK_TRY(r);
             h->launches++;

@@ -40,32 +40,22 @@ namespace fdk {
 template <typename E>
 struct TmaCfg;
 // Tile and pipeline shapes (macros for tuning sweeps).  Measured on the 2048^3 / 4096-view
-// workload, 128 views per launch: mixed R 12 -> 16 and 4 -> 8 views per stage 1985 -> 2215 GUPS
-// (more stages changed nothing; R >= 20 spills); FP32 R 8 -> 12: 1007 -> 1051 GUPS.  Unrolling
-// the view loop (1641 GUPS) and pairing two views per slice with an FP16 pre-add (2115 GUPS)
-// were slower: both raise register pressure past the 2-CTA budget.  Three CTAs per SM (72
-// registers; FDK_TMA_MIN_BLOCKS=3) were slower too: R 12 with 4 or 6 views per stage 2003 /
-// 1960 GUPS, R 8 with 4 views 1830 GUPS -- the per-column setup amortised over fewer slices costs
-// more than the extra warps gain.  Prefetching a tile's volume runs a few view chunks before its
-// end (a branch inside the view loop) instead of at its start measured 11% slower (2168 against
-// 2421 GUPS at 512-view batches), though the loop's registers did not change.
+// workload with the first MIXED form of this kernel (FP16 mirror pairs gathered straight from
+// 36 x 40 boxes, 8 views per stage; replaced by the interpolation layout below), 128 views per
+// launch: mixed R 12 -> 16 and 4 -> 8 views per stage 1985 -> 2215 GUPS (more stages changed
+// nothing; R >= 20 spills); FP32 R 8 -> 12: 1007 -> 1051 GUPS.  Unrolling the view loop (1641
+// GUPS) and pairing two views per slice with an FP16 pre-add (2115 GUPS) were slower: both raise
+// register pressure past the 2-CTA budget.  Three CTAs per SM (72 registers;
+// FDK_TMA_MIN_BLOCKS=3) were slower too: R 12 with 4 or 6 views per stage 2003 / 1960 GUPS, R 8
+// with 4 views 1830 GUPS -- the per-column setup amortised over fewer slices costs more than the
+// extra warps gain.  Prefetching a tile's volume runs a few view chunks before its end (a branch
+// inside the view loop) instead of at its start measured 11% slower (2168 against 2421 GUPS at
+// 512-view batches), though the loop's registers did not change.  A layout with two detector
+// columns per 8-byte element (read by 64-bit loads) measured slower than that FP16 gather: 2133
+// against 2257 GUPS (its doubled boxes halved the views per stage and the kernel spilled).
 #ifndef FDK_TMA_MIXED_R
 #define FDK_TMA_MIXED_R 16
 #endif
-#ifndef FDK_TMA_MIXED_S
-#define FDK_TMA_MIXED_S 2
-#endif
-#ifndef FDK_TMA_MIXED_NV
-#define FDK_TMA_MIXED_NV 8
-#endif
-template <>
-struct TmaCfg<__half2> {
-    static constexpr int R = FDK_TMA_MIXED_R;    // top-slab slices per thread
-    static constexpr int BW = 36;                // box width (v elements), 144 B rows
-    static constexpr int BH = 40;                // box height (u rows)
-    static constexpr int NV = FDK_TMA_MIXED_NV;  // views per stage
-    static constexpr int S = FDK_TMA_MIXED_S;    // stages
-};
 #ifndef FDK_TMA_FP32_R
 #define FDK_TMA_FP32_R 12
 #endif
@@ -89,8 +79,7 @@ struct __align__(8) HalfLerp {
     __half2 a, d;
 };
 // Measured on the 2048^3 / 4096-view workload, 512-view batches, conversion included: 2644
-// against 2339 GUPS for the FP16 gather on one box (5 views per stage: slower).  The tile height
-// is the FP16 kernel's, so both cut the slab into the same z tiles and bands.
+// against 2339 GUPS for the FP16 gather it replaced, on one box.
 #ifndef FDK_TMA_LERP_NV
 #define FDK_TMA_LERP_NV 4
 #endif
@@ -105,7 +94,7 @@ struct __align__(8) HalfLerp {
 #endif
 template <>
 struct TmaCfg<HalfLerp> {
-    static constexpr int R = TmaCfg<__half2>::R;
+    static constexpr int R = FDK_TMA_MIXED_R;  // top-slab slices per thread
     static constexpr int BW = FDK_TMA_LERP_BW;  // 34: 272 B rows, 68 words, an 8-row bank period for 8-byte loads
     static constexpr int BH = FDK_TMA_LERP_BH;
     static constexpr int NV = FDK_TMA_LERP_NV;
@@ -159,11 +148,6 @@ __host__ __device__ constexpr int tma_smem_bytes() {
     return TmaCfg<E>::S * TmaCfg<E>::NV * (tma_box_bytes<E>() + (int)sizeof(TmaMeta)) + 2 * TmaCfg<E>::S * 8;
 }
 
-__device__ __forceinline__ unsigned lds32(unsigned addr) {
-    unsigned v;
-    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(addr));
-    return v;
-}
 __device__ __forceinline__ float2 lds64f(unsigned addr) {
     float2 v;
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
@@ -175,31 +159,6 @@ __device__ __forceinline__ uint2 lds64u(unsigned addr) {
     return v;
 }
 __device__ __forceinline__ __half2 u2h(unsigned u) { return *reinterpret_cast<__half2 *>(&u); }
-// The four FP16 mirror pairs of one bilinear sample: (u0, vi), (u0, vi+1), (u0+1, vi), (u0+1, vi+1)
-// from a staged box (address a of (u0, vi), row_bytes apart) or from the global view.  (A layout
-// with two rows per 8-byte element, read by 64-bit loads, measured slower: 2133 against 2257 GUPS
-// on the C3 workload -- its doubled boxes halve the views per stage and the kernel spills.)
-template <typename E>
-struct HalfGather;
-template <>
-struct HalfGather<__half2> {
-    static constexpr unsigned ESZ = 4;
-    __device__ static __forceinline__ void smem(unsigned a, unsigned row_bytes, __half2 &e0, __half2 &e1, __half2 &e2,
-                                                __half2 &e3) {
-        e0 = u2h(lds32(a));
-        e1 = u2h(lds32(a + 4));
-        e2 = u2h(lds32(a + row_bytes));
-        e3 = u2h(lds32(a + row_bytes + 4));
-    }
-    __device__ static __forceinline__ void global(const void *gview, long long i, int nv, __half2 &e0, __half2 &e1,
-                                                  __half2 &e2, __half2 &e3) {
-        const unsigned *g0 = reinterpret_cast<const unsigned *>(gview) + i;
-        e0 = u2h(__ldg(g0));
-        e1 = u2h(__ldg(g0 + 1));
-        e2 = u2h(__ldg(g0 + nv));
-        e3 = u2h(__ldg(g0 + nv + 1));
-    }
-};
 __device__ __forceinline__ void acc_add_f16x2(float &lo_acc, float &hi_acc, __half2 r) {
     // sm_100 mixed-precision add (measured faster than converting the pair and adding in FP32)
     const unsigned u = *reinterpret_cast<unsigned *>(&r);
@@ -343,76 +302,6 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
             const __half2 l0 = __hfma2(g, u2h(p0.y), u2h(p0.x));
             const __half2 l1 = __hfma2(g, u2h(p1.y), u2h(p1.x));
             const float2 rf = __half22float2(__hfma2(l1, bw, __hmul2(l0, aw)));
-            if (mv) am[k] += rf.x;
-            if (rv) ar[k] += rf.y;
-        }
-    } else if constexpr (!std::is_same<E, float2>::value) {
-        using G = HalfGather<E>;
-        constexpr unsigned RB = C::BW * G::ESZ;  // box row bytes
-        const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
-        if (md.staged) {
-            // fixed point: t = (v - v_lo) * 1024 + 1.5 * 2^23; bits = 0x4B400000 + round(1024 (v - v_lo))
-            const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
-            const float B1 = B * 1024.f;
-            const unsigned rowp = box + (unsigned)(u0 - md.u_lo) * RB - (0x4B400000u >> 10) * G::ESZ;
-            if (md.interior) {
-#pragma unroll
-                for (int k = 0; k < R; k++) {
-                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
-                    const unsigned a = rowp + (bits >> 10) * G::ESZ;
-                    const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
-                    __half2 e0, e1, e2, e3;
-                    G::smem(a, RB, e0, e1, e2, e3);
-                    const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
-                    const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
-                    const __half2 d = __hsub2(c1, c0);
-                    const __half2 r = __hfma2(fvh, d, __hsub2(c0, d));
-                    acc_add_f16x2(am[k], ar[k], r);
-                }
-            } else {
-                // slices near the detector's top or bottom edge: the bounds rule of SUBPIXEL per
-                // slice (v and its mirror nv-1-v in [0, nv-1)), the same fixed-point gather inside
-#pragma unroll
-                for (int k = 0; k < R; k++) {
-                    const float v = fmaf(B, (float)k, A);
-                    const float vr = (float)(nv - 1) - v;
-                    const bool mv = v >= 0.f && v < (float)(nv - 1);
-                    const bool rv = vr >= 0.f && vr < (float)(nv - 1);
-                    if (!(mv || rv)) continue;
-                    const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
-                    const unsigned a = rowp + (bits >> 10) * G::ESZ;
-                    const __half2 fvh = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));
-                    __half2 e0, e1, e2, e3;
-                    G::smem(a, RB, e0, e1, e2, e3);
-                    const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
-                    const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
-                    const __half2 d = __hsub2(c1, c0);
-                    const float2 rf = __half22float2(__hfma2(fvh, d, __hsub2(c0, d)));
-                    if (mv) am[k] += rf.x;
-                    if (rv) ar[k] += rf.y;
-                }
-            }
-            return;
-        }
-#pragma unroll
-        for (int k = 0; k < R; k++) {
-            const float v = fmaf(B, (float)k, A);
-            const float vr = (float)(nv - 1) - v;
-            const bool mv = v >= 0.f && v < (float)(nv - 1);
-            const bool rv = vr >= 0.f && vr < (float)(nv - 1);
-            if (!(mv || rv)) continue;
-            const float vf = fminf(floorf(v), (float)(nv - 2));
-            const int vi = (int)vf;
-            const __half2 fv2 = __float2half2_rn(v - vf);
-            __half2 e0, e1, e2, e3;
-            if (md.staged)
-                G::smem(box + (unsigned)(u0 - md.u_lo) * RB + (unsigned)(vi - md.v_lo) * G::ESZ, RB, e0, e1, e2, e3);
-            else
-                G::global(gview, (long long)u0 * nv + vi, nv, e0, e1, e2, e3);
-            const __half2 c0 = __hfma2(e2, bw, __hmul2(e0, aw));
-            const __half2 c1 = __hfma2(e3, bw, __hmul2(e1, aw));
-            __half2 r = __hfma2(fv2, __hsub2(c1, c0), c0);
-            const float2 rf = __half22float2(r);
             if (mv) am[k] += rf.x;
             if (rv) ar[k] += rf.y;
         }
