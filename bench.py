@@ -702,8 +702,8 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
         if traffic is not None and nvox != 2048 ** 3:
             traffic *= nvox / 2048 ** 3  # recorded for 2048^3 (scaled by voxel count from a 512^3 capture)
         et = '__half2' if args.precision == 'mixed' else 'float2'
-        staged = ("bp_tma_kernel<HalfLerp> (views converted to the interpolation layout)" if args.precision == "mixed"
-                  else f"bp_tma_kernel<{et}>")
+        staged = ("bp_tma_kernel<HalfLerp*> (views converted to the interpolation layout; compact boxes where "
+                  "every tile fits)" if args.precision == "mixed" else f"bp_tma_kernel<{et}>")
         roofline = {
             "kernel": {"quarter-turn": f"bp_sym_kernel<{et}> (views paired with their quarter-turn partners)",
                        "staged": staged, "exact": "bp_exact_kernel"}[bp_kind],

@@ -248,6 +248,9 @@ struct fdk_bp {
     long long lerp_call_cap = 0;
     cudaEvent_t lerp_call_ev = nullptr;
     bool lerp_call_used = false;
+    // the reconstructor's MIXED launches read through the compact boxes (every tile fits them)
+    bool lerp_compact = false;
+    bool lerp_compact_ok = false;  // the compact kernel runs at the same grid
     ListRec *h_list = nullptr, *d_list = nullptr;
     cudaEvent_t list_ev[kListRing] = {};
     bool list_used[kListRing] = {};
@@ -525,6 +528,44 @@ bool quarter_turn_holds(const float *mats, int n_proj, int n, int nz, int rot) {
     return true;
 }
 
+// Every staged tile (16 x 16 columns of the sub-box x R slices; the first and last z tiles of the
+// top slab bound the rest, as in sym_footprints_fit) fits a BW x BH box in every checked view
+// (all views, or 256 spread over the scan), by the producer's box rule (tile_box) in double with
+// one element of slack for its FP32 rounding.  A footprint that does not fit is still
+// backprojected, through global memory, so this only picks the faster box.
+bool lerp_compact_fits(const float *mats, int n_proj, const BpFastPlan &p, int R, int BW, int BH) {
+    const int tiles_x = (p.nxs + 15) / 16, tiles_y = (p.nys + 15) / 16;
+    const int last = (int)((ceil_div(p.nzz, R) - 1) * R);
+    const int step = std::max(1, n_proj / 256);
+    for (int j = 0; j < n_proj; j += step) {
+        const float *m = mats + 12 * (long long)j;
+        for (int tx = 0; tx < tiles_x; tx++)
+            for (int ty = 0; ty < tiles_y; ty++)
+                for (int e = 0; e < 2; e++) {
+                    const double xa = p.x0 + tx * 16, xb = p.x0 + std::min(tx * 16 + 16, p.nxs) - 1;
+                    const double ya = p.y0 + ty * 16, yb = p.y0 + std::min(ty * 16 + 16, p.nys) - 1;
+                    const double za = p.z0 + (e ? last : 0), zb = za + R - 1;
+                    double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+                    for (int c = 0; c < 4; c++) {
+                        const double x = (c & 1) ? xb : xa, y = (c & 2) ? yb : ya;
+                        const double rw = 1.0 / ((double)m[8] * x + (double)m[9] * y + (double)m[11]);
+                        const double U = ((double)m[0] * x + (double)m[1] * y + (double)m[3]) * rw;
+                        const double vw = (double)m[4] * x + (double)m[5] * y + (double)m[7];
+                        const double va = ((double)m[6] * za + vw) * rw, vb = ((double)m[6] * zb + vw) * rw;
+                        umin = std::min(umin, U);
+                        umax = std::max(umax, U);
+                        vmin = std::min(vmin, std::min(va, vb));
+                        vmax = std::max(vmax, std::max(va, vb));
+                    }
+                    const double ulo = std::max(std::floor(umin) - 1, -1.0), uhi = std::min(std::floor(umax) + 2, (double)p.nu);
+                    const double vlo = std::max(std::floor(vmin) - 1, -8.0), vhi = std::min(std::floor(vmax) + 2, p.nv + 4.0);
+                    const long long v_lo = ((long long)vlo) & ~3ll;
+                    if ((long long)uhi - (long long)ulo + 1 > BH - 1 || (long long)vhi - v_lo + 1 > BW - 1) return false;
+                }
+    }
+    return true;
+}
+
 // Every tile of the quadrant (16 x 16 columns x R slices of the top slab [z0, z0 + nzz)) fits
 // the kernel's BW x BH box in every view (each view is the base of a quadruple).  The map is linear-fractional, so a tile's
 // extremes sit at its corner columns; the box's u extent (floor(umax) + 2 - (floor(umin) - 1) + 1)
@@ -645,6 +686,11 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
             if (h->plan.tma_ok) {
                 s = precision == FDK_BP_MIXED ? tma_prepare<HalfLerp>(h->plan.tma_ctas, device)
                                               : tma_prepare<float2>(h->plan.tma_ctas, device);
+                if (s == FDK_OK && precision == FDK_BP_MIXED) {
+                    int c = 0;
+                    s = tma_prepare<HalfLerpCompact>(c, device);
+                    h->lerp_compact_ok = s == FDK_OK && c == h->plan.tma_ctas;
+                }
                 if (s == FDK_OK) ck(cudaMalloc(&h->plan.d_err, sizeof(unsigned int)), "error word");
                 if (s == FDK_OK) ck(cudaMemsetAsync(h->plan.d_err, 0, sizeof(unsigned int), h->stream), "error word");
                 if (s == FDK_OK)
@@ -959,6 +1005,22 @@ int fdk_bp_reserve_lerp_internal(fdk_bp *h, int n_slots) {
     FDK_ABI_END
 }
 
+// The reconstructor's scan (every view's matrix): MIXED list launches read through the compact
+// boxes when every tile fits them (lerp_compact_fits).  Before the first launch.  Internal to the
+// library (recon.cu).
+int fdk_bp_choose_lerp_box_internal(fdk_bp *h, const float *mats, int n_proj) {
+    FDK_CHECK_ARG(h && mats && n_proj > 0, "NULL argument or no views");
+    h->lerp_compact = false;
+    if (h->precision != FDK_BP_MIXED || !h->plan.tma_ok || !h->lerp_compact_ok || h->launches > 0) return FDK_OK;
+    if (check_circular(mats, n_proj) != FDK_OK) {
+        clear_error();
+        return FDK_OK;
+    }
+    using C = TmaCfg<HalfLerpCompact>;
+    h->lerp_compact = lerp_compact_fits(mats, n_proj, h->plan, C::R, C::BW, C::BH);
+    return FDK_OK;
+}
+
 // Device scalar multiplying the MIXED accumulators of device-resident FP16 views (their
 // producer divided the filtered values by it).  Internal to the library (recon.cu).
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale) {
@@ -1161,7 +1223,11 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 const size_t frame = (size_t)h->plan.nu * h->plan.nv * esz;
                 const void *pv = static_cast<const char *>(lv ? (const void *)lv : views) + frame * s_slot[s0];
                 const long long m0 = 12 * (long long)s_view[s0];
-                FDK_TRY(lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
+                FDK_TRY(lv && h->lerp_compact
+                            ? bp_tma_launch<HalfLerpCompact>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0,
+                                                             host_mats + m0, ns, st, acc_scale, h->band_tz[k],
+                                                             h->band_tz[k + 1])
+                        : lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
                                                      ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
                         : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0, ns,
                                                 st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
@@ -1178,7 +1244,11 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 vl.view[i] = s_view[s0 + i];
             }
             FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(ViewList), cudaMemcpyHostToDevice, st));
-            const int r = lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns, st,
+            const int r = lv && h->lerp_compact
+                              ? bp_tma_launch<HalfLerpCompact>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns,
+                                                               st, acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl,
+                                                               &dev->views, n_slots)
+                          : lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns, st,
                                                        acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
                                                        n_slots)
                           : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,

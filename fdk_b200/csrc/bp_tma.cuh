@@ -100,6 +100,21 @@ struct TmaCfg<HalfLerp> {
     static constexpr int NV = FDK_TMA_LERP_NV;
     static constexpr int S = FDK_TMA_LERP_S;
 };
+// The same layout read through shorter boxes with 5 views per stage, for geometries where every
+// tile's footprint fits them (chosen on the host: lerp_compact_fits).  On one B200: 2768 against
+// 2718 GUPS at 2048^3, but 1077 against 2499 at 1024^3 from 1536 x 1024 views, where half the
+// footprints do not fit and are gathered from global memory.
+struct __align__(8) HalfLerpCompact : HalfLerp {};
+template <>
+struct TmaCfg<HalfLerpCompact> {
+    static constexpr int R = FDK_TMA_MIXED_R;
+    static constexpr int BW = 34;
+    static constexpr int BH = 32;
+    static constexpr int NV = 5;
+    static constexpr int S = 2;
+};
+template <typename E>
+constexpr bool is_lerp_v = std::is_same<E, HalfLerp>::value || std::is_same<E, HalfLerpCompact>::value;
 
 struct __align__(16) TmaMeta {
     float m[12];
@@ -244,7 +259,7 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
     const float fu = U - fuf;
     const int u0 = (int)fuf;
 
-    if constexpr (std::is_same<E, HalfLerp>::value) {
+    if constexpr (is_lerp_v<E>) {
         constexpr unsigned RB = C::BW * 8;  // box row bytes
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
         if (md.staged) {

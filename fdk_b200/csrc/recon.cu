@@ -82,6 +82,7 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                              const int *q_view, int n_quad, void *stream, int band);
 int fdk_bp_set_acc_scale_internal(fdk_bp *h, const float *d_scale);
 int fdk_bp_reserve_lerp_internal(fdk_bp *h, int n_slots);
+int fdk_bp_choose_lerp_box_internal(fdk_bp *h, const float *mats, int n_proj);
 long long fdk_bp_launches_internal(const fdk_bp *h);
 int fdk_bp_bp_device_mats_internal(fdk_bp *h, const void *dev_proj, int32_t layout, const float *dev_mats,
                                    int32_t n_proj, const float *host_mats, void *stream, int32_t band);
@@ -433,6 +434,8 @@ int fdk_recon_create_slab(fdk_recon **out, const fdk_geometry *g, int64_t top_z,
         if (s == FDK_OK) s = fdk_bp_sym_setup_internal(h->bp, h->mats.data(), (int)g->n_proj, &h->sym_rot);
         // MIXED: the staged kernel reads each batch converted to the interpolation layout
         if (s == FDK_OK && precision == FDK_BP_MIXED) s = fdk_bp_reserve_lerp_internal(h->bp, h->batch);
+        if (s == FDK_OK && precision == FDK_BP_MIXED)
+            s = fdk_bp_choose_lerp_box_internal(h->bp, h->mats.data(), (int)g->n_proj);
     }
     if (s == FDK_OK) s = wait_stream(h->compute, h->sync_ev[0], "fdk_recon_create");  // set-up copies landed
     if (s != FDK_OK) {
