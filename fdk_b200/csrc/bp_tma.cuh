@@ -100,17 +100,22 @@ struct TmaCfg<HalfLerp> {
     static constexpr int NV = FDK_TMA_LERP_NV;
     static constexpr int S = FDK_TMA_LERP_S;
 };
-// The same layout read through shorter boxes with 5 views per stage, for geometries where every
-// tile's footprint fits them (chosen on the host: lerp_compact_fits).  On one B200: 2768 against
-// 2718 GUPS at 2048^3, but 1077 against 2499 at 1024^3 from 1536 x 1024 views, where half the
-// footprints do not fit and are gathered from global memory.
+// The same layout read through shorter boxes with more views per stage, for geometries where
+// every tile's footprint fits them (chosen on the host: lerp_compact_fits).  On one B200, 5 views
+// per stage: 2768 against 2718 GUPS at 2048^3, but 1077 against 2499 at 1024^3 from 1536 x 1024
+// views, where half the footprints do not fit and are gathered from global memory.  Views per
+// stage at 2048^3 / 512^3: 4 2727 / 2651, 5 2774 / 2696, 6 2792 / 2721 (7 would not leave room
+// for two CTAs per SM).
 struct __align__(8) HalfLerpCompact : HalfLerp {};
+#ifndef FDK_TMA_COMPACT_NV
+#define FDK_TMA_COMPACT_NV 6
+#endif
 template <>
 struct TmaCfg<HalfLerpCompact> {
     static constexpr int R = FDK_TMA_MIXED_R;
     static constexpr int BW = 34;
     static constexpr int BH = 32;
-    static constexpr int NV = 5;
+    static constexpr int NV = FDK_TMA_COMPACT_NV;
     static constexpr int S = 2;
 };
 template <typename E>
