@@ -79,7 +79,9 @@ struct __align__(8) HalfLerp {
     __half2 a, d;
 };
 // Measured on the 2048^3 / 4096-view workload, 512-view batches, conversion included: 2644
-// against 2339 GUPS for the FP16 gather it replaced, on one box.
+// against 2339 GUPS for the FP16 gather it replaced, on one box.  5 views per stage: 2528 against
+// 2502 GUPS at 1024^3 (C4), but 1868 against 1961 for the drop-in's 32-view calls, whose last
+// stage is then partial; 4 kept.
 #ifndef FDK_TMA_LERP_NV
 #define FDK_TMA_LERP_NV 4
 #endif
