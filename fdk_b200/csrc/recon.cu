@@ -62,6 +62,10 @@ struct fdk_recon {
     int cur = 0;
     int pending = 0;
     bool held = false;
+    // first batch of a scan streamed from host memory (staged precisions, batches of 128 or more):
+    // 0 = not decided (no view since creation or reset), 1 = filling a quarter-size first batch,
+    // launched as soon as it is full, 2 = regular batches
+    int ramp = 0;
     std::vector<int> bviews[2];
     int sym_rot = 0;  // quarter-turn kernel's column map (0: not available for this scan)
     double filter_ms = 0;
@@ -222,6 +226,7 @@ int flush_all(fdk_recon *h) {
     }
     h->held = false;
     h->pending = 0;
+    if (h->ramp == 1) h->ramp = 2;
     h->bviews[0].clear();
     h->bviews[1].clear();
     return FDK_OK;
@@ -231,13 +236,19 @@ int flush_all(fdk_recon *h) {
 // filling batch behind the views already there; a full batch is held until the next one starts
 // (rotate_full).  FP32_EXACT: views join a batch only when they continue the waiting views (the
 // next view expected); otherwise everything waiting is backprojected first.  Staged precisions:
-// any views join.
-int process_chunk(fdk_recon *h, const float *d_src, const int64_t *ids, int n, cudaEvent_t release) {
+// any views join.  host: the views came from host memory (a scan that starts so begins with a
+// quarter-size batch).
+int process_chunk(fdk_recon *h, const float *d_src, const int64_t *ids, int n, cudaEvent_t release, bool host) {
     const fdk_geometry &g = h->g;
     const long long frame = g.nu * g.nv;
     const long long dstride = h->layout == FDK_LAYOUT_MIRROR ? 2 * frame : frame;
     const size_t esz = h->dtype == FDK_DTYPE_F16 ? 2 : 4;
     const bool exact = h->precision == FDK_BP_FP32_EXACT;
+    // A scan pushed from host memory starts with a quarter-size batch, backprojected as soon as
+    // it is full, so the backprojection starts while the rest of the scan is still crossing PCIe
+    // (a full first batch would be held until the next one starts).
+    if (h->ramp == 0) h->ramp = (host && !exact && h->batch >= 128) ? 1 : 2;
+    const int ramp_n = h->batch / 4;
     for (int done = 0; done < n;) {
         if (exact && (h->pending > 0 || h->held)) {
             const long long expected = h->pending > 0 ? (long long)h->bviews[h->cur].back() + 1
@@ -246,6 +257,7 @@ int process_chunk(fdk_recon *h, const float *d_src, const int64_t *ids, int n, c
         }
         if (h->pending == h->batch) FDK_TRY(rotate_full(h));
         int m = std::min(n - done, h->batch - h->pending);
+        if (h->ramp == 1) m = std::min(m, ramp_n - h->pending);
         if (exact) {  // one consecutive run at a time
             int r = 1;
             while (r < m && ids[done + r] == ids[done + r - 1] + 1) r++;
@@ -269,6 +281,15 @@ int process_chunk(fdk_recon *h, const float *d_src, const int64_t *ids, int n, c
         h->ftimers.push_back(t);
         h->pending += m;
         done += m;
+        if (h->ramp == 1 && h->pending == ramp_n) {
+            // the first batch goes now; the next fills the other buffer (its filters queue behind
+            // this launch on the compute stream)
+            FDK_TRY(launch_batch(h, h->cur, h->pending, -1));
+            h->cur ^= 1;
+            h->pending = 0;
+            h->bviews[h->cur].clear();
+            h->ramp = 2;
+        }
     }
     if (h->ftimers.size() > 256) FDK_TRY(collect_filter_timers(h));
     // the raw views are consumed once filtered
@@ -298,7 +319,7 @@ int push_host(fdk_recon *h, const float *host_views, const int64_t *ids, int64_t
                                  cudaMemcpyHostToDevice, h->copy));
         FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
         FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
-        FDK_TRY(process_chunk(h, h->d_raw[k], ids + c, m, h->raw_free[k]));
+        FDK_TRY(process_chunk(h, h->d_raw[k], ids + c, m, h->raw_free[k], true));
         last = h->raw_ready[k];
     }
     // the caller may reuse host_views once its last copy has landed
@@ -521,7 +542,7 @@ int fdk_recon_push_folder(fdk_recon *h, const char *folder, int64_t first, int64
         FDK_CUDA(cudaEventRecord(h->raw_ready[k], h->copy));
         FDK_CUDA(cudaStreamWaitEvent(h->compute, h->raw_ready[k], 0));
         const std::vector<int64_t> ids = consecutive(first + c, m);
-        FDK_TRY(process_chunk(h, h->d_raw[k], ids.data(), m, h->raw_free[k]));
+        FDK_TRY(process_chunk(h, h->d_raw[k], ids.data(), m, h->raw_free[k], true));
     }
     return FDK_OK;
     FDK_ABI_END
@@ -533,7 +554,7 @@ int push_device_ids(fdk_recon *h, const float *dev_views, const int64_t *ids, in
     const int cap = h->precision == FDK_BP_FP32_EXACT ? std::min(h->batch, 32) : h->batch;
     for (long long c = 0; c < n; c += cap) {
         const int m = (int)std::min<long long>(cap, n - c);
-        FDK_TRY(process_chunk(h, dev_views + c * frame, ids + c, m, nullptr));
+        FDK_TRY(process_chunk(h, dev_views + c * frame, ids + c, m, nullptr, false));
     }
     return FDK_OK;
 }
@@ -670,6 +691,7 @@ int fdk_recon_reset(fdk_recon *h) {
     h->filter_launches = 0;
     h->pending = 0;  // filtered views not yet backprojected are dropped with the volume
     h->held = false;
+    h->ramp = 0;
     h->bviews[0].clear();
     h->bviews[1].clear();
     h->cur = 0;

@@ -361,3 +361,27 @@ def test_mixed_tiles_that_miss_their_box_read_global_memory():
     e32 = rel_l2(vols["fp32"][m], f64[m])
     print("mixed vs fp64", e64, "fp32 vs fp64", e32)
     assert e64 <= 1e-3 and e32 <= 1e-5
+
+
+def test_host_scan_starts_with_a_quarter_batch():
+    """A scan pushed from host memory with batches of 128 views backprojects its first 32 views
+    as soon as they are filtered (the backprojection starts while the rest is still being
+    copied); pushed from device memory, the first batch waits for 128.  Both give the same
+    volume up to FP32 summation order."""
+    import torch
+
+    n, views = 48, 160
+    p = small_param(n, 64, 64, views)
+    _, proj = phantom_views(p, seed=13)
+    dev = torch.from_numpy(proj).cuda()
+    h = F.Reconstructor(p, "fp32", batch=128)
+    d = F.Reconstructor(p, "fp32", batch=128)
+    h.push(proj[:40].copy(), 0)
+    d.push_device(dev.data_ptr(), 0, 40)
+    assert h.launch_count > d.launch_count  # the early batch's backprojection launches
+    h.push(proj[40:].copy(), 40)
+    d.push_device(dev[40:].data_ptr(), 40, views - 40)
+    vh, vd = h.volume(), d.volume()
+    h.close()
+    d.close()
+    assert rel_l2(vh, vd) <= 1e-6
