@@ -122,6 +122,13 @@ struct TmaCfg<HalfLerpCompact> {
 };
 template <typename E>
 constexpr bool is_lerp_v = std::is_same<E, HalfLerp>::value || std::is_same<E, HalfLerpCompact>::value;
+// Whether a kernel gathers the views of a tile whose footprint exceeds its box from global
+// memory.  The compact-box kernel runs only where the host found that every footprint fits
+// (lerp_compact_fits, with slack for rounding), so it has no such path: it skips such a view and
+// sets the device error word (kErrFootprint), never silently, and keeps the registers the path
+// would take.
+template <typename E>
+constexpr bool has_global_fallback_v = !std::is_same<E, HalfLerpCompact>::value;
 
 struct __align__(16) TmaMeta {
     float m[12];
@@ -306,6 +313,7 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
             }
             return;
         }
+        if constexpr (!has_global_fallback_v<E>) return;  // reported by the producer
         // a tile whose footprint does not fit the box: the column's two detector rows from global
         // memory (row pointer formed once; rare, and kept lean so the hot loops above keep their
         // registers)
@@ -514,9 +522,13 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
                 }
                 __syncwarp();
                 if (lane == 0) {
-                    unsigned n_staged = 0;
+                    unsigned n_staged = 0, n_views = 0;
                     for (int l = 0; l < NV; l++)
-                        if (c * NV + l < a.n_proj && meta[s * NV + l].staged) n_staged++;
+                        if (c * NV + l < a.n_proj) {
+                            n_views++;
+                            if (meta[s * NV + l].staged) n_staged++;
+                        }
+                    if (!has_global_fallback_v<E> && n_staged != n_views) atomicOr(a.err, kErrFootprint);
                     mbar_arrive_tx(full0 + 8 * s, n_staged * BOX_TX);
                     for (int l = 0; l < NV; l++) {
                         const TmaMeta &md = meta[s * NV + l];
