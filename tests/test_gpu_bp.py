@@ -140,9 +140,11 @@ def test_fast_border_views(precision, kernel, nu, nv, monkeypatch):
     got = run_bp(precision, p, top, bot, [filt], [mats])
     want = oracle_bp_ref32(top, bot[5], n, [filt], [mats])
     m = knife_edge_mask(p, top, bot[5])
+    e = rel_l2(got[m], want[m])
+    print(precision, kernel, nu, nv, "rel-L2 vs reference arithmetic", e)
     # MIXED on white-noise views: FP16 samples and the 1/1024-pixel fixed-point fraction of the
     # staged gather bound the per-sample error at a few 1e-4 of the sample differences
-    assert rel_l2(got[m], want[m]) <= (1e-5 if precision == "fp32" else 1.5e-3), rel_l2(got[m], want[m])
+    assert e <= (1e-5 if precision == "fp32" else 1.5e-3), e
 
 
 def test_fast_rejects_non_circular_matrices():
