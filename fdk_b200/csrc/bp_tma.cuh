@@ -17,7 +17,8 @@
 //    (4 mod 32) spreads them over the banks (measured model: ~1.2 wavefronts per gather,
 //    against 2.9 for 16 x 2 lanes with pitch 24).
 //  * FP16 path: v is carried in fixed point, t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per
-//    voxel.  The integer part of t's bits indexes the box; the low 10 bits are the fraction,
+//    voxel, with the per-view constants of that form folded into the stage metadata by the
+//    producer (fold_lerp_meta).  The integer part of t's bits indexes the box; the low 10 bits are the fraction,
 //    which OR-ed under the FP16 exponent of 1.0 gives 1 + fv as a half directly.  The two
 //    u-lerps use weights (1-fu) w and fu w folded in, the v-lerp is one HFMA2 over the
 //    (voxel, mirror) pair, and the result is added to FP32 accumulators with the sm_100
@@ -137,6 +138,20 @@ struct __align__(16) TmaMeta {
 };
 static_assert(sizeof(TmaMeta) == 64 && offsetof(TmaMeta, u_lo) == 48, "load_meta reads TmaMeta as 4 x 16 B");
 
+// In the lerp kernels the producer rewrites m[] for the tile once per view (fold_lerp_meta), so
+// a consumer's per-column setup shrinks to the arithmetic that depends on its column:
+//   m[0..2]  (m0, m1, m3) s           U = (m[0] x + m[1] y + m[2]) rw
+//   m[3..5]  (m8, m9, m11) s          rw = 1 / (m[3] x + m[4] y + m[5]); weight rw^2
+//   m[6..8]  (m4, m5, m6 z0 + m7) 1024 s   with z0 the tile's first slice
+//   m[9]     m6 1024 s                fixed-point v step per slice: m[9] rw
+//   m[10]    1.5 2^23 - 1024 v_lo     fixed point of the first slice: (m[6] x + m[7] y + m[8]) rw + m[10]
+//   m[11]    (bits) shared address of the view's box, less u_lo rows and the fixed-point offset
+// s = wscale^-1/2 is a power of two (weight_scale), so the scaled rows give U, v and rw^2 wscale
+// bit for bit as the unscaled ones give U, v and rw^2 times wscale.  Against the consumer-side
+// setup (I2F, FADD and FMULs per column and view for the fixed point, the weight and the box row):
+// register spill 16 -> 4 bytes (compact boxes), 2945 -> 3079 GUPS at 2048^3 in 512-view batches,
+// both builds measured twice on one B200.
+
 struct BpTmaArgs {
     float *vol;
     float *comp;
@@ -147,7 +162,8 @@ struct BpTmaArgs {
     int n_proj, nu, nv;
     int x0, y0, z0, nxs, nys, nzz;
     long long D;
-    float wscale;
+    float wscale;  // a power of four (weight_scale)
+    float wsinv;   // wscale^-1/2, a power of two
     int tiles_x, tiles_y, tiles_z;
     int tz0;  // first z tile of this launch (a launch may cover a band of z tiles)
     unsigned long long wait_ns;  // limit of every mbarrier wait (FDK_BP_WAIT_NS, default 10 s)
@@ -253,6 +269,19 @@ __device__ __forceinline__ void tile_box(const float *m, float xa, float xb, flo
     md.interior = (vmin > 1e-3f && vmax < (float)(nv - 1) - 1e-3f) ? 1 : 0;
 }
 
+// The lerp kernels' form of a view's metadata (layout above TmaMeta): m is the view's matrix in
+// registers, za the tile's first slice, box the shared address of the view's box, s = wscale^-1/2.
+template <typename E>
+__device__ __forceinline__ void fold_lerp_meta(const float (&m)[12], float za, unsigned box, float s, TmaMeta &md) {
+    constexpr unsigned RB = TmaCfg<E>::BW * 8;  // box row bytes
+    const float s10 = s * 1024.f;
+    const float f[12] = {m[0] * s,   m[1] * s,   m[3] * s,   m[8] * s,  m[9] * s, m[11] * s, m[4] * s10, m[5] * s10,
+                         fmaf(m[6], za, m[7]) * s10, m[6] * s10, 12582912.f - 1024.f * (float)md.v_lo,
+                         __uint_as_float(box - (unsigned)md.u_lo * RB - (0x4B400000u >> 10) * 8u)};
+#pragma unroll
+    for (int q = 0; q < 12; q++) md.m[q] = f[q];
+}
+
 // One view's contribution to a thread's column: R voxel pairs.
 template <typename E>
 __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, const E *gview, float x, float y,
@@ -262,25 +291,24 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
     constexpr int R = C::R;
     const MetaRegs md = load_meta(md_s);
     const float *m = md.m;
-    const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
-    const float rw = __fdividef(1.0f, w);
-    const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
-    const float A = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], zf0, m[7]))) * rw;  // v at the run's first slice
-    const float B = m[6] * rw;                                                  // dv per slice
-    const float wt = rw * rw * wscale;
-    if (!(U >= 0.f && U < (float)(nu - 1))) return;  // every sample of this column is zero
-    const float fuf = floorf(U);
-    const float fu = U - fuf;
-    const int u0 = (int)fuf;
-
     if constexpr (is_lerp_v<E>) {
+        // metadata folded by the producer (fold_lerp_meta)
         constexpr unsigned RB = C::BW * 8;  // box row bytes
-        const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
+        const float rw = __fdividef(1.0f, fmaf(m[3], x, fmaf(m[4], y, m[5])));
+        const float U = fmaf(m[0], x, fmaf(m[1], y, m[2])) * rw;
+        if (!(U >= 0.f && U < (float)(nu - 1))) return;  // every sample of this column is zero
+        const float fuf = floorf(U);
+        const float fu = U - fuf;
+        const int u0 = (int)fuf;
+        const float wt = rw * rw;
+        const float bwf = fu * wt;
+        const __half2 aw = __float2half2_rn(wt - bwf), bw = __float2half2_rn(bwf);
+        const float nv1024 = fmaf(m[6], x, fmaf(m[7], y, m[8]));  // 1024 (v at the run's first slice) / rw
         if (md.staged) {
-            // fixed point as in the FP16 gather: bits = 0x4B400000 + round(1024 (v - v_lo))
-            const float C0 = fmaf(A - (float)md.v_lo, 1024.f, 12582912.f);
-            const float B1 = B * 1024.f;
-            const unsigned rowp = box + (unsigned)(u0 - md.u_lo) * RB - (0x4B400000u >> 10) * 8u;
+            // fixed point: bits = 0x4B400000 + round(1024 (v - v_lo)); the box row of u0 is m[11] + u0 rows
+            const float C0 = fmaf(nv1024, rw, m[10]);
+            const float B1 = m[9] * rw;
+            const unsigned rowp = __float_as_uint(m[11]) + (unsigned)u0 * RB;
             if (md.interior) {
 #pragma unroll
                 for (int k = 0; k < R; k++) {
@@ -293,6 +321,7 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
                     acc_add_f16x2(am[k], ar[k], __hfma2(l1, bw, __hmul2(l0, aw)));
                 }
             } else {
+                const float A = nv1024 * rw * (1.0f / 1024.f), B = B1 * (1.0f / 1024.f);  // v in pixels
 #pragma unroll
                 for (int k = 0; k < R; k++) {
                     const float v = fmaf(B, (float)k, A);
@@ -317,6 +346,7 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
         // a tile whose footprint does not fit the box: the column's two detector rows from global
         // memory (row pointer formed once; rare, and kept lean so the hot loops above keep their
         // registers)
+        const float A = nv1024 * rw * (1.0f / 1024.f), B = m[9] * rw * (1.0f / 1024.f);
         const uint2 *grow = reinterpret_cast<const uint2 *>(gview) + (long long)u0 * nv;
 #pragma unroll
         for (int k = 0; k < R; k++) {
@@ -335,43 +365,53 @@ __device__ __forceinline__ void column_view(const TmaMeta &md_s, unsigned box, c
             if (mv) am[k] += rf.x;
             if (rv) ar[k] += rf.y;
         }
-    } else {
-        const float wa = (1.f - fu) * wt, wb = fu * wt;
+        return;
+    }
+    const float w = fmaf(m[8], x, fmaf(m[9], y, m[11]));
+    const float rw = __fdividef(1.0f, w);
+    const float U = fmaf(m[0], x, fmaf(m[1], y, m[3])) * rw;
+    const float A = fmaf(m[4], x, fmaf(m[5], y, fmaf(m[6], zf0, m[7]))) * rw;  // v at the run's first slice
+    const float B = m[6] * rw;                                                  // dv per slice
+    const float wt = rw * rw * wscale;
+    if (!(U >= 0.f && U < (float)(nu - 1))) return;  // every sample of this column is zero
+    const float fuf = floorf(U);
+    const float fu = U - fuf;
+    const int u0 = (int)fuf;
+    const float wa = (1.f - fu) * wt, wb = fu * wt;
 #pragma unroll
-        for (int k = 0; k < R; k++) {
-            const float v = fmaf(B, (float)k, A);
-            bool mv = true, rv = true;
-            float vf;
-            if (!(md.staged && md.interior)) {
-                const float vr = (float)(nv - 1) - v;
-                mv = v >= 0.f && v < (float)(nv - 1);
-                rv = vr >= 0.f && vr < (float)(nv - 1);
-                if (!(mv || rv)) continue;
-                vf = fminf(floorf(v), (float)(nv - 2));
-            } else {
-                vf = floorf(v);
-            }
-            const int vi = (int)vf;
-            const float fv = v - vf;
-            float2 e0, e1, e2, e3;
-            if (md.staged) {
-                const unsigned a = box + (unsigned)(((u0 - md.u_lo) * C::BW + (vi - md.v_lo)) * 8);
-                e0 = lds64f(a);
-                e1 = lds64f(a + 8);
-                e2 = lds64f(a + C::BW * 8);
-                e3 = lds64f(a + C::BW * 8 + 8);
-            } else {
-                const float2 *g0 = reinterpret_cast<const float2 *>(gview) + (long long)u0 * nv + vi;
-                e0 = __ldg(g0);
-                e1 = __ldg(g0 + 1);
-                e2 = __ldg(g0 + nv);
-                e3 = __ldg(g0 + nv + 1);
-            }
-            const float c0x = fmaf(e2.x, wb, e0.x * wa), c0y = fmaf(e2.y, wb, e0.y * wa);
-            const float c1x = fmaf(e3.x, wb, e1.x * wa), c1y = fmaf(e3.y, wb, e1.y * wa);
-            if (mv) am[k] += fmaf(fv, c1x - c0x, c0x);
-            if (rv) ar[k] += fmaf(fv, c1y - c0y, c0y);
+    for (int k = 0; k < R; k++) {
+        const float v = fmaf(B, (float)k, A);
+        bool mv = true, rv = true;
+        float vf;
+        if (!(md.staged && md.interior)) {
+            const float vr = (float)(nv - 1) - v;
+            mv = v >= 0.f && v < (float)(nv - 1);
+            rv = vr >= 0.f && vr < (float)(nv - 1);
+            if (!(mv || rv)) continue;
+            vf = fminf(floorf(v), (float)(nv - 2));
+        } else {
+            vf = floorf(v);
         }
+        const int vi = (int)vf;
+        const float fv = v - vf;
+        float2 e0, e1, e2, e3;
+        if (md.staged) {
+            const unsigned a = box + (unsigned)(((u0 - md.u_lo) * C::BW + (vi - md.v_lo)) * 8);
+            e0 = lds64f(a);
+            e1 = lds64f(a + 8);
+            e2 = lds64f(a + C::BW * 8);
+            e3 = lds64f(a + C::BW * 8 + 8);
+        } else {
+            const float2 *g0 = reinterpret_cast<const float2 *>(gview) + (long long)u0 * nv + vi;
+            e0 = __ldg(g0);
+            e1 = __ldg(g0 + 1);
+            e2 = __ldg(g0 + nv);
+            e3 = __ldg(g0 + nv + 1);
+        }
+        const float c0x = fmaf(e2.x, wb, e0.x * wa), c0y = fmaf(e2.y, wb, e0.y * wa);
+        const float c1x = fmaf(e3.x, wb, e1.x * wa), c1y = fmaf(e3.y, wb, e1.y * wa);
+        if (mv) am[k] += fmaf(fv, c1x - c0x, c0x);
+        if (rv) ar[k] += fmaf(fv, c1y - c0y, c0y);
     }
 }
 
@@ -512,9 +552,16 @@ __global__ void __launch_bounds__(288, FDK_TMA_MIN_BLOCKS)
                     TmaMeta &md = meta[s * NV + lane];
                     if (view < a.n_proj) {
                         const float *mg = a.mats + 12 * (long long)(a.list_view ? __ldg(a.list_view + view) : view);
+                        float mr[12];
 #pragma unroll
-                        for (int q = 0; q < 12; q++) md.m[q] = __ldg(mg + q);
-                        tile_box<E>(md.m, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
+                        for (int q = 0; q < 12; q++) mr[q] = __ldg(mg + q);
+                        tile_box<E>(mr, xa, xb, ya, yb, za, zb, a.nu, a.nv, md);
+                        if constexpr (is_lerp_v<E>) {
+                            fold_lerp_meta<E>(mr, za, boxes + (s * NV + lane) * BOX, a.wsinv, md);
+                        } else {
+#pragma unroll
+                            for (int q = 0; q < 12; q++) md.m[q] = mr[q];
+                        }
                     } else {
                         md.staged = 0;
                         md.interior = 0;
@@ -642,10 +689,13 @@ inline int bp_test_withhold() {
     return (e && atoi(e) == 1) ? 1 : 0;
 }
 
-// Square of the source distance of the volume centre in view 0: keeps f^2 * wscale near 1.
+// Square of the source distance of the volume centre in view 0, rounded to a power of four
+// (within a factor of two of it): keeps f^2 * wscale near 1, and its square root is a power of
+// two, so scaling by it is exact (fold_lerp_meta folds wscale^-1/2 into the matrix rows).
 inline float weight_scale(const float *host_mats, float xc, float yc) {
     const float w = host_mats[8] * xc + host_mats[9] * yc + host_mats[11];
-    return (w > 0.f) ? w * w : 1.0f;
+    if (!(w > 0.f)) return 1.0f;
+    return ldexpf(1.0f, 2 * (int)lrintf(log2f(w)));
 }
 
 // Backproject n views into the z tiles [tz_begin, tz_end) of R top slices each (with their
@@ -687,6 +737,7 @@ inline int bp_tma_launch(const BpFastPlan &p, float *vol, float *comp, const voi
     a.D = p.D;
     a.wscale = weight_scale(host_mats + (list ? 12 * (long long)list->view[0] : 0), p.x0 + 0.5f * (p.nxs - 1),
                             p.y0 + 0.5f * (p.nys - 1));
+    a.wsinv = ldexpf(1.0f, -ilogbf(a.wscale) / 2);  // exact: wscale is a power of four
     a.tiles_x = (int)ceil_div(p.nxs, 16);
     a.tiles_y = (int)ceil_div(p.nys, 16);
     const int tz_all = (int)ceil_div(p.nzz, C::R);
