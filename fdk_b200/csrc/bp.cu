@@ -135,28 +135,60 @@ __global__ void transpose_views_kernel(const float *__restrict__ src, float *__r
     }
 }
 
-// Gather listed voxels (x, y, z of the whole volume) from the slab-pair volume [x][y][zs];
-// voxels outside the handle's boxes read NaN.  MIXED folds its compensation term.
-// MIRROR FP16 views -> the interpolation layout (HalfLerp): d = E(v+1) - E(v) rounded to FP16,
-// a = E(v) - d rounded, so a + d reproduces E(v) to one FP16 rounding; d = 0 at v = nv-1.
+// Largest magnitude of the FP16 values of n half2 pairs, as the bits of a non-negative float
+// (as absmax_kernel).  16-byte loads; pairs past the last whole group of four one by one.
+__global__ void absmax_half2_kernel(const __half2 *__restrict__ x, long long n, unsigned int *out) {
+    float m = 0.f;
+    const long long n4 = n / 4;
+    const uint4 *x4 = reinterpret_cast<const uint4 *>(x);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const uint4 q = x4[i];
+        const unsigned w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&w[j]));
+            m = fmaxf(m, fmaxf(fabsf(f.x), fabsf(f.y)));
+        }
+    }
+    for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float2 f = __half22float2(x[i]);
+        m = fmaxf(m, fmaxf(fabsf(f.x), fabsf(f.y)));
+    }
+    for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__device__ __forceinline__ float pow2i(int e) { return __int_as_float((127 + e) << 23); }  // -126 <= e <= 127
+
+// MIRROR FP16 views -> the interpolation layout (HalfLerp), scaled by 2^-k with 2^k just above
+// the batch's largest magnitude M (absmax): e = E(v) 2^-k (exact unless it falls below the FP16
+// normal range), d = (E(v+1) - E(v)) 2^(14-k) rounded to FP16 (|d| < 2^15; 0 at v = nv-1).  A
+// sample at v + fv is then e + (fv 2^-14) d, fv 2^-14 being the FP16 subnormal whose mantissa
+// is the fixed-point fraction, so the sample carries the roundings of E(v) and of d only.
+// out_scale = acc_scale (1 if null) * 2^k, the accumulator scale of the launches that read dst.
 __global__ void to_lerp_kernel(const __half2 *__restrict__ src, HalfLerp *__restrict__ dst, long long rows,
-                               int nv) {
+                               int nv, const unsigned int *absmax, const float *acc_scale, float *out_scale) {
+    const float M = __uint_as_float(*absmax);
+    const int k = (M > 0.f && M < 65536.f) ? ilogbf(M) + 1 : 0;  // M is an FP16 magnitude: -23 <= k <= 16
+    const float se = pow2i(-k), sd = pow2i(14 - k);
+    if (blockIdx.x == 0 && threadIdx.x == 0) *out_scale = (acc_scale ? *acc_scale : 1.0f) * pow2i(k);
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         const __half2 *s = src + r * nv;
         HalfLerp *d = dst + r * nv;
         for (int v = threadIdx.x; v < nv; v += blockDim.x) {
             const float2 e0 = __half22float2(s[v]);
             const float2 e1 = v + 1 < nv ? __half22float2(s[v + 1]) : e0;
-            const __half2 dh = __floats2half2_rn(e1.x - e0.x, e1.y - e0.y);
-            const float2 df = __half22float2(dh);
             HalfLerp o;
-            o.a = __floats2half2_rn(e0.x - df.x, e0.y - df.y);
-            o.d = dh;
+            o.e = __floats2half2_rn(e0.x * se, e0.y * se);
+            o.d = __floats2half2_rn((e1.x - e0.x) * sd, (e1.y - e0.y) * sd);
             d[v] = o;
         }
     }
 }
 
+// Gather listed voxels (x, y, z of the whole volume) from the slab-pair volume [x][y][zs];
+// voxels outside the handle's boxes read NaN.  MIXED folds its compensation term.
 __global__ void sample_voxels_kernel(const float *__restrict__ vol, const float *__restrict__ comp,
                                      const int *__restrict__ xyz, long long n, float *__restrict__ out, int x0,
                                      int y0, int nxs, int nys, long long tz0, long long td, long long bz0,
@@ -209,6 +241,9 @@ struct fdk_bp {
     long long bp_count = 0;
     double kernel_ms = 0;
     BpFastPlan plan;
+    // MIXED: word 0 the largest |value| of the f32 views of a call; words 1-3 that of the FP16
+    // views of interpolation-layout buffer 0, 1 and the calls' buffer, words 5-7 (as floats) the
+    // accumulator scales of the launches that read those buffers (to_lerp_kernel)
     unsigned int *d_absmax = nullptr;
     const float *ext_scale = nullptr;  // accumulator scale of FP16 views pushed by the reconstructor
     // The staged kernel runs each batch as n_bands launches over bands of z tiles (top slices
@@ -292,7 +327,31 @@ int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
 //   kernels without bands run whole with band 0 and do nothing for the others)
 // The n MIRROR FP16 views of a BackProjectionFDK call converted to the interpolation layout on
 // st (after the previous call's launches, which may have read the buffer on another stream).
-int lerp_call_views(fdk_bp *h, const void *dev_proj, int n, cudaStream_t st, HalfLerp **out) {
+// The largest-magnitude word (j: 0, 1 the list buffers, 2 the calls' buffer) and the accumulator
+// scale of interpolation-layout buffer j.
+unsigned int *lerp_absmax(fdk_bp *h, int j) { return h->d_absmax + 1 + j; }
+float *lerp_scale(fdk_bp *h, int j) { return reinterpret_cast<float *>(h->d_absmax + 5 + j); }
+
+// n_views MIRROR FP16 views at src -> the interpolation layout at dst (buffer j): their largest
+// magnitude, then the scaled conversion, on st.
+int convert_lerp(fdk_bp *h, const void *src, HalfLerp *dst, long long n_views, int j, const float *acc_scale,
+                 cudaStream_t st) {
+    FDK_CHECK_ARG(((uintptr_t)src & 15) == 0, "views must start on a 16-byte boundary");
+    const long long rows = n_views * h->plan.nu;
+    const long long pairs = rows * h->plan.nv;
+    FDK_CUDA(cudaMemsetAsync(lerp_absmax(h, j), 0, sizeof(unsigned int), st));
+    absmax_half2_kernel<<<(int)std::min<long long>(ceil_div(pairs / 4 + 1, 256), 148 * 8), 256, 0, st>>>(
+        static_cast<const __half2 *>(src), pairs, lerp_absmax(h, j));
+    FDK_CUDA(cudaGetLastError());
+    to_lerp_kernel<<<(int)std::min<long long>(rows, 148 * 16), 256, 0, st>>>(
+        static_cast<const __half2 *>(src), dst, rows, h->plan.nv, lerp_absmax(h, j), acc_scale, lerp_scale(h, j));
+    FDK_CUDA(cudaGetLastError());
+    h->launches += 2;
+    return FDK_OK;
+}
+
+int lerp_call_views(fdk_bp *h, const void *dev_proj, int n, cudaStream_t st, const float *acc_scale, HalfLerp **out,
+                    const float **scale) {
     const long long frame = (long long)h->plan.nu * h->plan.nv;
     if (!h->lerp_call_ev) FDK_CUDA(cudaEventCreateWithFlags(&h->lerp_call_ev, cudaEventDisableTiming));
     if (h->lerp_call_cap < n) {
@@ -304,12 +363,9 @@ int lerp_call_views(fdk_bp *h, const void *dev_proj, int n, cudaStream_t st, Hal
         h->lerp_call_cap = n;
     }
     if (h->lerp_call_used) FDK_CUDA(cudaStreamWaitEvent(st, h->lerp_call_ev, 0));
-    const long long rows = (long long)n * h->plan.nu;
-    to_lerp_kernel<<<(int)std::min<long long>(rows, 148 * 16), 256, 0, st>>>(static_cast<const __half2 *>(dev_proj),
-                                                                           h->d_lerp_call, rows, h->plan.nv);
-    FDK_CUDA(cudaGetLastError());
-    h->launches++;
+    FDK_TRY(convert_lerp(h, dev_proj, h->d_lerp_call, n, 2, acc_scale, st));
     *out = h->d_lerp_call;
+    *scale = lerp_scale(h, 2);
     return FDK_OK;
 }
 
@@ -354,11 +410,12 @@ int launch_bp(fdk_bp *h, const void *dev_proj, int layout, int transpose, const 
         if (h->plan.tma_ok && ((uintptr_t)dev_proj & 15) == 0) {
             // MIXED: the views once in the interpolation layout, read by every band's launch
             HalfLerp *lv = nullptr;
-            if (h->precision == FDK_BP_MIXED) FDK_TRY(lerp_call_views(h, dev_proj, n, st, &lv));
+            const float *lerp_sc = nullptr;
+            if (h->precision == FDK_BP_MIXED) FDK_TRY(lerp_call_views(h, dev_proj, n, st, acc_scale, &lv, &lerp_sc));
             for (int k = kb; k < ke; k++) {
                 if (lv)
                     FDK_TRY(bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, n, st,
-                                                    acc_scale, h->band_tz[k], h->band_tz[k + 1]));
+                                                    lerp_sc, h->band_tz[k], h->band_tz[k + 1]));
                 else
                     FDK_TRY(bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, dev_proj, d_mats, host_mats, n, st,
                                                   acc_scale, h->band_tz[k], h->band_tz[k + 1]));
@@ -671,7 +728,7 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         const size_t esz = precision == FDK_BP_MIXED ? sizeof(__half2) : sizeof(float2);
         ck(cudaMalloc(&h->d_mirror, esz * frame * proj_count), "mirror staging");
         if (s == FDK_OK && precision == FDK_BP_MIXED) {
-            ck(cudaMalloc(&h->d_absmax, sizeof(unsigned int)), "absmax");
+            ck(cudaMalloc(&h->d_absmax, sizeof(unsigned int) * 8), "absmax");  // + the lerp words (lerp_word)
             ck(cudaMalloc(&h->d_comp, sizeof(float) * nvox), "compensation");
             if (s == FDK_OK) ck(cudaMemsetAsync(h->d_comp, 0, sizeof(float) * nvox, h->stream), "compensation zero");
         }
@@ -720,7 +777,8 @@ int fdk_bp_create(fdk_bp **out, int32_t proj_width, int32_t proj_height, int32_t
         const void *kernels[] = {(const void *)transform_volume_kernel<true>,
                                  (const void *)transform_volume_kernel<false>, (const void *)absmax_kernel,
                                  (const void *)to_mirror_half_kernel, (const void *)to_mirror_kernel<float2>,
-                                 (const void *)fold_comp_kernel, (const void *)to_lerp_kernel};
+                                 (const void *)fold_comp_kernel, (const void *)to_lerp_kernel,
+                                 (const void *)absmax_half2_kernel};
         for (const void *kf : kernels)
             if (s == FDK_OK) ck(cudaFuncGetAttributes(&fa, kf), "kernel load");
     }
@@ -1113,7 +1171,8 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
 namespace {
 // The interpolation-layout copy of slots 0..n_slots-1 of a MIXED views buffer: converted on st
 // when the first (or only) band of a batch is launched (band <= 0), reused by its later bands.
-int lerp_views(fdk_bp *h, const void *views, int n_slots, int band, cudaStream_t st, HalfLerp **out) {
+int lerp_views(fdk_bp *h, const void *views, int n_slots, int band, cudaStream_t st, const float *acc_scale,
+               HalfLerp **out, const float **scale) {
     FDK_CHECK_ARG(h->lerp_slots >= n_slots, "interpolation-layout buffers of %lld views for a batch of %d",
                   h->lerp_slots, n_slots);
     int j = h->lerp_src[0] == views ? 0 : h->lerp_src[1] == views ? 1 : -1;
@@ -1122,14 +1181,11 @@ int lerp_views(fdk_bp *h, const void *views, int n_slots, int band, cudaStream_t
             j = h->lerp_next;
             h->lerp_next ^= 1;
         }
-        const long long rows = (long long)n_slots * h->plan.nu;
-        to_lerp_kernel<<<(int)std::min<long long>(rows, 148 * 16), 256, 0, st>>>(
-            static_cast<const __half2 *>(views), h->d_lerp[j], rows, h->plan.nv);
-        FDK_CUDA(cudaGetLastError());
-        h->launches++;
+        FDK_TRY(convert_lerp(h, views, h->d_lerp[j], n_slots, j, acc_scale, st));
         h->lerp_src[j] = views;
     }
     *out = h->d_lerp[j];
+    *scale = lerp_scale(h, j);
     return FDK_OK;
 }
 
@@ -1181,12 +1237,13 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
     FDK_TRY(take_timer(h, tm));
     FDK_CUDA(cudaEventRecord(tm.first, st));
     HalfLerp *lv = nullptr;
+    const float *lerp_sc = nullptr;  // accumulator scale of the launches that read lv
     if (mixed) {
         int used = 0;  // slots the launches read (a partial batch converts only its own)
         for (int i = 0; i < n_single; i++) used = std::max(used, s_slot[i] + 1);
         for (int i = 0; i < 4 * n_quad; i++) used = std::max(used, q_slot[i] + 1);
         FDK_CHECK_ARG(used <= n_slots, "slot outside the views buffer");
-        FDK_TRY(lerp_views(h, views, used, band, st, &lv));
+        FDK_TRY(lerp_views(h, views, used, band, st, acc_scale, &lv, &lerp_sc));
     }
     for (int k = kb; k < ke; k++) {
         for (int q0 = 0; q0 < n_quad; q0 += kSymMaxQuads) {
@@ -1203,7 +1260,7 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
             FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(SymQuads), cudaMemcpyHostToDevice, st));
             const int r = mixed ? bp_sym_launch<HalfLerp>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, lv, n_slots,
                                                           d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
-                                                          acc_scale, h->band_z[k], h->band_z[k + 1])
+                                                          lerp_sc, h->band_z[k], h->band_z[k + 1])
                                 : bp_sym_launch<float2>(h->plan, h->sym_ctas, h->d_vol, h->d_comp, views, n_slots,
                                                         d_mats, host_mats, sq, &dev->quads, nq, h->sym_rot, st,
                                                         acc_scale, h->band_z[k], h->band_z[k + 1]);
@@ -1225,10 +1282,10 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
                 const long long m0 = 12 * (long long)s_view[s0];
                 FDK_TRY(lv && h->lerp_compact
                             ? bp_tma_launch<HalfLerpCompact>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0,
-                                                             host_mats + m0, ns, st, acc_scale, h->band_tz[k],
+                                                             host_mats + m0, ns, st, lerp_sc, h->band_tz[k],
                                                              h->band_tz[k + 1])
                         : lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0,
-                                                     ns, st, acc_scale, h->band_tz[k], h->band_tz[k + 1])
+                                                     ns, st, lerp_sc, h->band_tz[k], h->band_tz[k + 1])
                         : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, pv, d_mats + m0, host_mats + m0, ns,
                                                 st, acc_scale, h->band_tz[k], h->band_tz[k + 1]));
                 h->launches++;
@@ -1246,10 +1303,10 @@ int fdk_bp_bp_lists_internal(fdk_bp *h, const void *views, int n_slots, const fl
             FDK_CUDA(cudaMemcpyAsync(dev, rec, sizeof(ViewList), cudaMemcpyHostToDevice, st));
             const int r = lv && h->lerp_compact
                               ? bp_tma_launch<HalfLerpCompact>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns,
-                                                               st, acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl,
+                                                               st, lerp_sc, h->band_tz[k], h->band_tz[k + 1], &vl,
                                                                &dev->views, n_slots)
                           : lv ? bp_tma_launch<HalfLerp>(h->plan, h->d_vol, h->d_comp, lv, d_mats, host_mats, ns, st,
-                                                       acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
+                                                       lerp_sc, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views,
                                                        n_slots)
                           : bp_tma_launch<float2>(h->plan, h->d_vol, h->d_comp, views, d_mats, host_mats, ns, st,
                                                   acc_scale, h->band_tz[k], h->band_tz[k + 1], &vl, &dev->views, n_slots);

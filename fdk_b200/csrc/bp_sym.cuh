@@ -20,8 +20,8 @@
 //    each member view's slot in the views buffer, into a ring of S stages completed by
 //    mbarrier expect_tx; consumers release a stage through a second mbarrier.
 //  * MIXED reads the views in the interpolation layout (HalfLerp, bp_tma.cuh): v in fixed point
-//    (t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per slice gives the box index and 1 + fv),
-//    and per member two 8-byte loads and a + (1 + fv) d per detector column, then the u-lerp;
+//    (t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per slice gives the box index and fv 2^-14),
+//    and per member two 8-byte loads and e + (fv 2^-14) d per detector column, then the u-lerp;
 //    the FP16 pair is added to the FP32 accumulators by the sm_100 mixed-precision add.
 //  * FP32: FP32 mirror pairs, the four bilinear weights formed once per slice, FFMA.
 //  * The host admits a launch only when every tile's footprint fits the box in every base view
@@ -206,7 +206,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
 
     if constexpr (std::is_same<E, HalfLerp>::value) {
         // one address, fraction and u-weight set per slice serves the four members: per member
-        // two 8-byte loads (the sample's two detector columns) and a + (1 + fv) d per column
+        // two 8-byte loads (the sample's two detector columns) and e + (fv 2^-14) d per column
         constexpr unsigned RB = C::BW * 8;
         const __half2 aw = __float2half2_rn((1.f - fu) * wt), bw = __float2half2_rn(fu * wt);
         const float C0 = fmaf(A - (float)v_lo, 1024.f, 12582912.f);
@@ -224,7 +224,7 @@ __device__ __forceinline__ void column_quad(const TmaMeta &md, unsigned box, flo
             }
             const unsigned bits = __float_as_uint(fmaf((float)k, B1, C0));
             const unsigned a = rowp + (bits >> 10) * 8u;
-            const __half2 g = __low2half2(u2h((bits & 0x3FFu) | 0x3C00u));  // 1 + fv
+            const __half2 g = __low2half2(u2h(bits & 0x3FFu));  // fv 2^-14 (FP16 subnormal)
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const uint2 p0 = lds64u(a + j * BOX), p1 = lds64u(a + j * BOX + RB);

@@ -143,8 +143,9 @@ def test_fast_border_views(precision, kernel, nu, nv, monkeypatch):
     e = rel_l2(got[m], want[m])
     print(precision, kernel, nu, nv, "rel-L2 vs reference arithmetic", e)
     # MIXED on white-noise views: FP16 samples and the 1/1024-pixel fixed-point fraction of the
-    # staged gather bound the per-sample error at a few 1e-4 of the sample differences
-    assert e <= (1e-5 if precision == "fp32" else 1.5e-3), e
+    # staged gather bound the per-sample error at a few 1e-4 of the sample differences; the
+    # north-star bar of 1e-3 holds even here, where neighbouring samples are uncorrelated
+    assert e <= (1e-5 if precision == "fp32" else 1e-3), e
 
 
 def test_fast_rejects_non_circular_matrices():
