@@ -49,7 +49,9 @@ struct TmaCfg;
 // register pressure past the 2-CTA budget.  Three CTAs per SM (72 registers;
 // FDK_TMA_MIN_BLOCKS=3) were slower too: R 12 with 4 or 6 views per stage 2003 / 1960 GUPS, R 8
 // with 4 views 1830 GUPS -- the per-column setup amortised over fewer slices costs more than the
-// extra warps gain.  Prefetching a tile's volume runs a few view chunks before its end (a branch
+// extra warps gain.  Again with the current MIXED kernel (folded per-view constants, scaled
+// interpolation layout; compact boxes of 4 views, 3 views in the 34 x 40 boxes, so that both
+// kernels hold three CTAs per SM): R 12 2648 and R 8 2130 against 3152 GUPS for R 16 at two.  Prefetching a tile's volume runs a few view chunks before its end (a branch
 // inside the view loop) instead of at its start measured 11% slower (2168 against 2421 GUPS at
 // 512-view batches), though the loop's registers did not change.  A layout with two detector
 // columns per 8-byte element (read by 64-bit loads) measured slower than that FP16 gather: 2133
@@ -203,6 +205,8 @@ __device__ __forceinline__ float2 lds64f(unsigned addr) {
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
     return v;
 }
+// (An ordinary C++ load through __cvta_shared_to_generic, which the compiler may schedule, measured
+// the same: 3131 against 3132 GUPS at 2048^3.)
 __device__ __forceinline__ uint2 lds64u(unsigned addr) {
     uint2 v;
     asm volatile("ld.shared.v2.b32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
