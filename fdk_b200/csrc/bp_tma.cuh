@@ -13,9 +13,9 @@
 //    (expect_tx).  Consumers release a stage through a second mbarrier.  No CTA-wide barrier
 //    is on the hot path, and no consumer instruction is spent on staging.
 //  * Warps 0-7 consume.  Lanes are an 8 x 4 block of voxel columns: their detector samples
-//    fall on about ten box rows at nearly the same v, and a row pitch of BW = 36 words
-//    (4 mod 32) spreads them over the banks (measured model: ~1.2 wavefronts per gather,
-//    against 2.9 for 16 x 2 lanes with pitch 24).
+//    fall on about ten box rows at nearly the same v, and a row pitch of 68 words (34 elements
+//    of 8 bytes, 4 mod 32) spreads them over the banks (ncu: 10% extra shared wavefronts,
+//    against 2.9 wavefronts per gather for 16 x 2 lanes with pitch 24).
 //  * FP16 path: v is carried in fixed point, t = (v - v_lo) * 1024 + 1.5 * 2^23, one FFMA per
 //    voxel, with the per-view constants of that form folded into the stage metadata by the
 //    producer (fold_lerp_meta).  The integer part of t's bits indexes the box; the low 10 bits
