@@ -215,9 +215,11 @@ using namespace fdk;
 namespace {
 // Most z bands per batch (tuning macro).  On the 2048^3 workload 8 bands against 4: the same
 // device time (2383 against 2386 GUPS) and e2e 2182 against 2117 GUPS, as the readback of the
-// last band, which no backprojection hides, halves.
+// last band, which no backprojection hides, halves.  16 against 8 with the current kernels
+// (64-slice bands, 221 tiles per persistent CTA): 3044 against 3014 GUPS and e2e 2776 against
+// 2743 (one box, each twice).
 #ifndef FDK_MAX_BANDS
-#define FDK_MAX_BANDS 8
+#define FDK_MAX_BANDS 16
 #endif
 constexpr int kMaxBands = FDK_MAX_BANDS;
 }
