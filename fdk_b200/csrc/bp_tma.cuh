@@ -115,7 +115,7 @@ struct TmaCfg<HalfLerp> {
 // per stage: 2768 against 2718 GUPS at 2048^3, but 1077 against 2499 at 1024^3 from 1536 x 1024
 // views, where half the footprints do not fit and are gathered from global memory.  Views per
 // stage at 2048^3 / 512^3: 4 2727 / 2651, 5 2774 / 2696, 6 2792 / 2721 (7 would not leave room
-// for two CTAs per SM).
+// for two CTAs per SM); with the current kernel at 2048^3, 5 views 3159 against 3171 GUPS for 6.
 struct __align__(8) HalfLerpCompact : HalfLerp {};
 #ifndef FDK_TMA_COMPACT_NV
 #define FDK_TMA_COMPACT_NV 6

@@ -9,7 +9,9 @@
 namespace fdk {
 
 constexpr long long kWaitLimit = 1ll << 26;
-// Sleep between a producer warp's polls of a stage's empty barrier (tuning macro; 0 = spin).
+// Sleep between a producer warp's polls of a stage's empty barrier (tuning macro; 0 = spin).  The
+// MIXED staged kernel at 2048^3 measured the same with 256 ns (3167 against 3171 GUPS): try_wait
+// already suspends the polling thread for a while before it reports an incomplete phase.
 #ifndef FDK_PRODUCER_SLEEP_NS
 #define FDK_PRODUCER_SLEEP_NS 0
 #endif
