@@ -327,8 +327,6 @@ int take_timer(fdk_bp *h, std::pair<cudaEvent_t, cudaEvent_t> &t) {
 //   layout MIRROR: mirror pairs (f32x2 or f16x2 per precision), proj_h rows x proj_w pairs
 //   band: -1 = every z band (the whole volume), else that band only (views counted with band 0;
 //   kernels without bands run whole with band 0 and do nothing for the others)
-// The n MIRROR FP16 views of a BackProjectionFDK call converted to the interpolation layout on
-// st (after the previous call's launches, which may have read the buffer on another stream).
 // The largest-magnitude word (j: 0, 1 the list buffers, 2 the calls' buffer) and the accumulator
 // scale of interpolation-layout buffer j.
 unsigned int *lerp_absmax(fdk_bp *h, int j) { return h->d_absmax + 1 + j; }
@@ -352,6 +350,9 @@ int convert_lerp(fdk_bp *h, const void *src, HalfLerp *dst, long long n_views, i
     return FDK_OK;
 }
 
+// The n MIRROR FP16 views of a BackProjectionFDK call converted to the interpolation layout on
+// st (after the previous call's launches, which may have read the buffer on another stream);
+// scale: the accumulator scale of the launches that read them.
 int lerp_call_views(fdk_bp *h, const void *dev_proj, int n, cudaStream_t st, const float *acc_scale, HalfLerp **out,
                     const float **scale) {
     const long long frame = (long long)h->plan.nu * h->plan.nv;
@@ -1172,7 +1173,8 @@ int fdk_bp_sym_setup_internal(fdk_bp *h, const float *mats, int n_proj, int *rot
 
 namespace {
 // The interpolation-layout copy of slots 0..n_slots-1 of a MIXED views buffer: converted on st
-// when the first (or only) band of a batch is launched (band <= 0), reused by its later bands.
+// when the first (or only) band of a batch is launched (band <= 0), reused by its later bands;
+// scale: the accumulator scale of the launches that read it (acc_scale times the copy's 2^k).
 int lerp_views(fdk_bp *h, const void *views, int n_slots, int band, cudaStream_t st, const float *acc_scale,
                HalfLerp **out, const float **scale) {
     FDK_CHECK_ARG(h->lerp_slots >= n_slots, "interpolation-layout buffers of %lld views for a batch of %d",
