@@ -311,6 +311,18 @@ def count_bp_batches(firsts, n: int, batch: int | None = None, contiguous: bool 
     return sizes
 
 
+def conversion_launches(precision: str) -> int:
+    """Launches a backprojection batch makes before its bands: MIXED finds the batch's largest
+    magnitude and converts its views to the interpolation layout."""
+    return 2 if precision == "mixed" else 0
+
+
+def band_launches(n_launches: int, steps: int, filter_per_step: int, n_batches: int, precision: str) -> float:
+    """Band launches per backprojection batch, from the library's launch count of a timed run:
+    each step's filter launches and each batch's conversion launches taken out."""
+    return (n_launches - steps * filter_per_step) / max(1, n_batches) - conversion_launches(precision)
+
+
 def l2_note(param, precision: str) -> str:
     """How the timed steps stand to the 126 MB L2: the volume (and the MIXED compensation) is
     read and written by every batch, so it decides whether a step can hit L2."""
@@ -692,9 +704,9 @@ def run_ours(args, param, rank: int, world: int, local: int) -> None:
             hbm_peak, hbm_src = mp["hbm_gbs"], "measured"
         except Exception:
             hbm_peak, hbm_src = 6650.0, "fallback"
-        # MIXED batches start with two conversion launches (largest magnitude, interpolation layout)
-        conv = 2 if args.precision == "mixed" else 0
-        bands = (n_launches - args.steps * (2 if filter_kind == "tensor" else 1)) / max(1, len(batch_sizes)) - conv
+        conv = conversion_launches(args.precision)
+        bands = band_launches(n_launches, args.steps, 2 if filter_kind == "tensor" else 1, len(batch_sizes),
+                              args.precision)
         # the staged kernel's DRAM bytes recorded by an ncu capture (MIXED: the interpolation layout)
         traffic = read_traffic("bp_tma_lerp_c2.md" if args.precision == "mixed" else f"bp_tma_{args.precision}_c2.md",
                                f"dram_bytes_per_{BATCH}_view_batch_full")

@@ -77,3 +77,12 @@ def test_metric_and_l2_note_follow_the_workload():
     assert bench.l2_note(c3, "mixed").startswith("inputs larger than L2")
     c1.nz = 64  # 16 MiB of volume state: smaller than L2
     assert bench.l2_note(c1, "fp32").startswith("inputs smaller than L2")
+
+
+def test_band_launches_from_the_launch_count():
+    # the driver's 20-step C3 run: 2 filter kernels per step, a 512- and a 128-view batch, each
+    # two conversion launches and 16 bands
+    assert bench.band_launches(20 * 2 + 2 * (2 + 16), 20, 2, 2, "mixed") == 16
+    # FP32 filters with one FFT launch per step and converts nothing
+    assert bench.band_launches(20 + 2 * 16, 20, 1, 2, "fp32") == 16
+    assert bench.conversion_launches("fp32_exact") == 0
