@@ -84,3 +84,18 @@ def test_ray_marcher_equals_reference():
         got = O.forward_project(v, q, a)
         assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 2e-5, i
         assert np.abs(got - want).max() <= 5e-5 * np.abs(want).max(), i
+
+
+import make_golden_gpu as MGG  # noqa: E402
+
+GG = np.load(os.path.join(HERE, "golden", "ref_gpu.npz"))
+
+
+def test_reference_cufft_filter_equals_oracle():
+    """The cuFFT plugin (CorrectImage_Real32 + FilterRow_Real32, pad = mean of 3) as it ran on a
+    B200, against the oracle's FP64 row filter with the same table and response."""
+    views = MGG.filter_views()
+    want = GG["flt_out"]
+    H = GG["flt_H"].astype(np.float64)
+    got = np.stack([O.filter_view(v, H, GG["flt_cos"], pad_n=3) for v in views])
+    assert np.abs(got - want).max() <= 5e-6 * np.abs(want).max()
