@@ -16,7 +16,7 @@
 //    slices); each consumer thread owns a base column and the three columns the quarter turns
 //    map it to, 2 x 4 x R FP32 accumulators (top and mirror slices of the four columns).
 //  * Warp 8 is the producer: per quadruple it computes the base view's footprint box of the
-//    tile (8 corners) and issues four 3-D TMA tile loads (no multicast) of that box, one from
+//    tile (8 corners) and issues four plain 3-D TMA tile loads of that box into its own CTA, one from
 //    each member view's slot in the views buffer, into a ring of S stages completed by
 //    mbarrier expect_tx; consumers release a stage through a second mbarrier.
 //  * MIXED reads the views in the interpolation layout (HalfLerp, bp_tma.cuh): v in fixed point
